@@ -1,0 +1,1013 @@
+// C-ABI implementation of include/bfps_b200.h (single GPU, sm_100a).
+//
+// The context owns every device buffer; one CUDA stream per context.
+// Kernels: passes.cuh (DNS step), particles.cuh (tracers), stats.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "bfps_b200.h"
+#include "particles.cuh"
+#include "passes.cuh"
+#include "stats.cuh"
+
+using namespace bfg;
+
+#define BFG_VERSION "bfps_b200 0.1 (sm_100a)"
+
+struct bfg_ctx {
+    int n = 0, nxv = 0, nxp = 0;
+    int real_bytes = 8;
+    int dealias = BFG_SMOOTH;
+    int device = 0;
+    double dkx = 1, dky = 1, dkz = 1;
+    double kM = 0, kM2 = 0, dk = 1, dk2 = 1;
+    int nshells = 0;
+    std::vector<double> kshell;
+    std::vector<int64_t> nshell;
+    // physics
+    double nu = 0.1;
+    int forcing = BFG_FORCING_NONE;
+    double famp = 1.0, fk0 = 2.0, fk1 = 4.0;
+    int fmode = 1;
+    int iteration = 0;
+    // device buffers
+    void* w0 = nullptr;  // state (cvorticity)
+    void* v1 = nullptr;
+    void* v2 = nullptr;
+    void* wa = nullptr;  // work / cvelocity
+    void* wb = nullptr;  // work
+    void* ru = nullptr;  // real velocity [z][y][x][3]
+    void* tw = nullptr;
+    void* filt = nullptr;
+    int nfilt = 1;
+    void* fac = nullptr;
+    double fac_dt = NAN, fac_nu = NAN;
+    void* stats_ws = nullptr;  // statistics partial sums
+    size_t stats_ws_bytes = 0;
+    size_t field_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t launches = 0;
+    std::string err;
+    // per-kernel profiling (bfg_profile)
+    bool prof = false;
+    std::vector<cudaEvent_t> prof_ev;  // start/stop pairs
+    std::vector<int> prof_kind;
+    size_t prof_used = 0;
+    double prof_ms[BFG_NKINDS] = {0};
+    int64_t prof_n[BFG_NKINDS] = {0};
+};
+
+struct bfg_pctx {
+    bfg_ctx* ctx = nullptr;
+    int64_t n = 0;
+    int neighbours = 1, smoothness = 1, nsteps = 1;
+    int step_idx = 1;
+    int head = 0;
+    bool rhs0_zero = true;
+    double* pos = nullptr;
+    double* hist = nullptr;
+    double* sample = nullptr;
+    std::vector<int64_t> idx;  // host copy of the global indices (device order)
+};
+
+// ------------------------------------------------------------ helpers --
+static int fail(bfg_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CU(call)                                                                      \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(c, BFG_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                          \
+    } while (0)
+
+static int after_launch(bfg_ctx* c, const char* what) {
+    c->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(c, BFG_ECUDA, "launch of %s: %s", what, cudaGetErrorString(e));
+    return 0;
+}
+
+// ----------------------------------------------------------- profiling --
+enum Kind { K_IZ = 0, K_IY = 1, K_X = 2, K_FY = 3, K_FZ = 4, K_KSPACE = 5, K_TRACER = 6, K_STATS = 7 };
+
+static void prof_flush(bfg_ctx* c) {
+    if (!c->prof_used) return;
+    cudaStreamSynchronize(c->stream);
+    for (size_t i = 0; i < c->prof_used; ++i) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]) == cudaSuccess) {
+            c->prof_ms[c->prof_kind[i]] += ms;
+            c->prof_n[c->prof_kind[i]] += 1;
+        }
+    }
+    c->prof_used = 0;
+}
+
+struct Prof {
+    bfg_ctx* c;
+    long slot = -1;
+    Prof(bfg_ctx* c_, int kind) : c(c_) {
+        if (!c->prof) return;
+        if (c->prof_used >= 4096) prof_flush(c);
+        if (c->prof_used == c->prof_kind.size()) {
+            cudaEvent_t a, b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            c->prof_ev.push_back(a);
+            c->prof_ev.push_back(b);
+            c->prof_kind.push_back(0);
+        }
+        slot = (long)c->prof_used++;
+        c->prof_kind[slot] = kind;
+        cudaEventRecord(c->prof_ev[2 * slot], c->stream);
+    }
+    ~Prof() {
+        if (slot >= 0) cudaEventRecord(c->prof_ev[2 * slot + 1], c->stream);
+    }
+};
+
+static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+static KParams kparams(const bfg_ctx* c, double dt) {
+    KParams k;
+    k.nxv = c->nxv;
+    k.nxp = c->nxp;
+    k.dkx = c->dkx;
+    k.dky = c->dky;
+    k.dkz = c->dkz;
+    k.kM2 = c->kM2;
+    k.dealias = c->dealias;
+    k.inv_dk2 = 1.0 / c->dk2;
+    k.nfilt = c->nfilt;
+    k.forcing = c->forcing;
+    k.famp = c->famp;
+    k.fk0 = c->fk0;
+    k.fk1 = c->fk1;
+    k.fmode = c->fmode;
+    k.dt = dt;
+    return k;
+}
+
+// cudaFuncSetAttribute once per kernel and device
+template <typename K>
+static cudaError_t ensure_smem(K kernel, size_t bytes, int device) {
+    static std::mutex mu;
+    static std::unordered_map<long long, bool> done;
+    const long long key = (long long)(uintptr_t)(void*)kernel * 64 + device;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count(key)) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)bytes);
+    if (e == cudaSuccess) done[key] = true;
+    return e;
+}
+
+static double kwrap_h(int i, int N, double dk) { return dk * (double)(i <= N / 2 ? i : i - N); }
+
+// ------------------------------------------------------------- engine --
+template <typename T, int N>
+struct Engine {
+    using C = cpx<T>;
+
+    template <int MODE>
+    static int col(bfg_ctx* c, double dt, const void* in0, const void* in1, void* out0,
+                   void* out1, const void* v0 = nullptr, const void* vp = nullptr,
+                   const void* fsrc = nullptr) {
+        constexpr int NB = col_nb(MODE);
+        constexpr int TKX = col_tkx<T, N, NB>();
+        constexpr size_t smem = col_smem_bytes<T, N, MODE>();
+        auto kern = col_pass<T, N, MODE>;
+        CU(ensure_smem(kern, smem, c->device));
+        dim3 grid((c->nxv + TKX - 1) / TKX, N);
+        constexpr int kind = (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) ? K_IZ
+                             : (MODE == CM_Y_INV1 || MODE == CM_Y_INV2)                  ? K_IY
+                             : (MODE == CM_Y_FWD1)                                      ? K_FY
+                                                                                        : K_FZ;
+        Prof pr(c, kind);
+        kern<<<grid, COL_THREADS, smem, c->stream>>>(
+            kparams(c, dt), (const C*)in0, (const C*)in1, (C*)out0, (C*)out1, (const C*)v0,
+            (const C*)vp, (const C*)fsrc, (const T*)c->filt, (const T*)c->fac,
+            (const C*)c->tw);
+        return after_launch(c, "col_pass");
+    }
+
+    template <int MODE, bool WRU>
+    static int row(bfg_ctx* c, const void* wu, const void* ww, void* wout, void* rout,
+                   const void* rin) {
+        constexpr size_t smem = row_smem_bytes<T, N, MODE>();
+        constexpr int ROWS = row_rows<T, N>();
+        auto kern = row_pass<T, N, MODE, WRU>;
+        CU(ensure_smem(kern, smem, c->device));
+        Prof pr(c, K_X);
+        row_pass<T, N, MODE, WRU><<<N * N / ROWS, ROW_THREADS, smem, c->stream>>>(
+            kparams(c, 0.0), (const C*)wu, (const C*)ww, (C*)wout, (T*)rout, (const T*)rin,
+            (const C*)c->tw);
+        return after_launch(c, "row_pass");
+    }
+
+    static int symmetrize(bfg_ctx* c, void* buf) {
+        Prof pr(c, K_KSPACE);
+        symmetrize_kernel<T, N><<<(N * N + 255) / 256, 256, 0, c->stream>>>((C*)buf, c->nxp);
+        return after_launch(c, "symmetrize");
+    }
+
+    static int stage(bfg_ctx* c, int s, double dt, bool write_ru) {
+        int rc;
+        const void* src = s == 0 ? c->w0 : (s == 1 ? c->v1 : c->v2);
+        if ((rc = col<CM_IZ_VEL>(c, dt, src, nullptr, c->wa, c->wb))) return rc;
+        if ((rc = col<CM_Y_INV2>(c, dt, c->wa, c->wb, c->wa, c->wb))) return rc;
+        if (write_ru) rc = row<RM_NONLIN, true>(c, c->wa, c->wb, c->wa, c->ru, nullptr);
+        else rc = row<RM_NONLIN, false>(c, c->wa, c->wb, c->wa, nullptr, nullptr);
+        if (rc) return rc;
+        if ((rc = col<CM_Y_FWD1>(c, dt, c->wa, nullptr, c->wa, nullptr))) return rc;
+        if (s == 0) return col<CM_FZ_RK1>(c, dt, c->wa, nullptr, c->v1, nullptr, c->w0, nullptr, src);
+        if (s == 1) return col<CM_FZ_RK2>(c, dt, c->wa, nullptr, c->v2, nullptr, c->w0, c->v1, src);
+        return col<CM_FZ_RK3>(c, dt, c->wa, nullptr, c->w0, nullptr, c->w0, c->v2, src);
+    }
+
+    static int finish_step(bfg_ctx* c) { return symmetrize(c, c->w0); }
+
+    static int velocity_state(bfg_ctx* c) {
+        const size_t npts = (size_t)N * N * c->nxv;
+        Prof pr(c, K_KSPACE);
+        velocity_kernel<T, N><<<(unsigned)((npts + 255) / 256), 256, 0, c->stream>>>(
+            kparams(c, 0.0), (const C*)c->w0, (C*)c->wa);
+        int rc = after_launch(c, "velocity");
+        if (rc) return rc;
+        return symmetrize(c, c->wa);
+    }
+
+    static int velocity_rspace(bfg_ctx* c) {
+        int rc;
+        if ((rc = col<CM_IZ_U>(c, 0.0, c->w0, nullptr, c->wb, nullptr))) return rc;
+        if ((rc = col<CM_Y_INV1>(c, 0.0, c->wb, nullptr, c->wb, nullptr))) return rc;
+        return row<RM_C2R, false>(c, c->wb, nullptr, nullptr, c->ru, nullptr);
+    }
+
+    static int fixup(bfg_ctx* c) {
+        int rc = symmetrize(c, c->w0);
+        if (rc) return rc;
+        const size_t npts = (size_t)N * N * c->nxv;
+        Prof pr(c, K_KSPACE);
+        lowpass_divfree_kernel<T, N><<<(unsigned)((npts + 255) / 256), 256, 0, c->stream>>>(
+            kparams(c, 0.0), (C*)c->w0);
+        return after_launch(c, "lowpass_divfree");
+    }
+
+    // unnormalised C2R of wb (state layout) into ru; uses wa
+    static int ift_wb(bfg_ctx* c) {
+        int rc;
+        if ((rc = col<CM_IZ_PLAIN>(c, 0.0, c->wb, nullptr, c->wa, nullptr))) return rc;
+        if ((rc = col<CM_Y_INV1>(c, 0.0, c->wa, nullptr, c->wa, nullptr))) return rc;
+        return row<RM_C2R, false>(c, c->wa, nullptr, nullptr, c->ru, nullptr);
+    }
+    // unnormalised R2C of ru into wb (state layout); uses wa
+    static int dft_ru(bfg_ctx* c) {
+        int rc;
+        if ((rc = row<RM_R2C, false>(c, nullptr, nullptr, c->wa, nullptr, c->ru))) return rc;
+        if ((rc = col<CM_Y_FWD1>(c, 0.0, c->wa, nullptr, c->wa, nullptr))) return rc;
+        return col<CM_FZ_PLAIN>(c, 0.0, c->wa, nullptr, c->wb, nullptr);
+    }
+
+    static int stats(bfg_ctx* c, const void* cfield, double max_est, int nbins, double* spec,
+                     double* mom, int64_t* hist);
+};
+
+#include "stats_engine.inl"
+
+// runtime dispatch over (T, N)
+template <template <typename, int> class F, typename... Args>
+static int dispatch(bfg_ctx* c, Args... args) {
+    if (c->real_bytes == 4) {
+        switch (c->n) {
+            case 16: return F<float, 16>::run(c, args...);
+            case 32: return F<float, 32>::run(c, args...);
+            case 64: return F<float, 64>::run(c, args...);
+            case 128: return F<float, 128>::run(c, args...);
+            case 256: return F<float, 256>::run(c, args...);
+            case 512: return F<float, 512>::run(c, args...);
+            case 1024: return F<float, 1024>::run(c, args...);
+        }
+    } else {
+        switch (c->n) {
+            case 16: return F<double, 16>::run(c, args...);
+            case 32: return F<double, 32>::run(c, args...);
+            case 64: return F<double, 64>::run(c, args...);
+            case 128: return F<double, 128>::run(c, args...);
+            case 256: return F<double, 256>::run(c, args...);
+            case 512: return F<double, 512>::run(c, args...);
+            case 1024: return F<double, 1024>::run(c, args...);
+        }
+    }
+    return fail(c, BFG_EUNSUP, "grid size %d not supported", c->n);
+}
+
+template <typename T, int N>
+struct OpStep {
+    static int run(bfg_ctx* c, double dt, bfg_pctx* p);
+};
+template <typename T, int N>
+struct OpVelocity {
+    static int run(bfg_ctx* c) { return Engine<T, N>::velocity_state(c); }
+};
+template <typename T, int N>
+struct OpVelocityR {
+    static int run(bfg_ctx* c) { return Engine<T, N>::velocity_rspace(c); }
+};
+template <typename T, int N>
+struct OpFixup {
+    static int run(bfg_ctx* c) { return Engine<T, N>::fixup(c); }
+};
+template <typename T, int N>
+struct OpIft {
+    static int run(bfg_ctx* c) { return Engine<T, N>::ift_wb(c); }
+};
+template <typename T, int N>
+struct OpDft {
+    static int run(bfg_ctx* c) { return Engine<T, N>::dft_ru(c); }
+};
+template <typename T, int N>
+struct OpStats {
+    static int run(bfg_ctx* c, const void* f, double me, int nb, double* s, double* m,
+                   int64_t* h) {
+        return Engine<T, N>::stats(c, f, me, nb, s, m, h);
+    }
+};
+
+// ------------------------------------------------------- host tables --
+template <typename T>
+static std::vector<T> host_twiddles(int N) {
+    std::vector<T> t(2 * (size_t)N);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int m = 0; m < N; ++m) {
+        const long double a = 2.0L * pi * (long double)m / (long double)N;
+        t[2 * m] = (T)cosl(a);
+        t[2 * m + 1] = (T)(-sinl(a));
+    }
+    return t;
+}
+
+static int upload_tables(bfg_ctx* c) {
+    const int N = c->n;
+    // twiddles exp(-2 pi i m / N)
+    if (c->real_bytes == 4) {
+        auto t = host_twiddles<float>(N);
+        CU(cudaMemcpy(c->tw, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice));
+    } else {
+        auto t = host_twiddles<double>(N);
+        CU(cudaMemcpy(c->tw, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // smooth dealias filter keyed by round(k2/dk2), filled in CLOOP order
+    // (kspace.cpp:109-137; later writes of a key win)
+    std::vector<double> filt;
+    if (c->dealias == BFG_SMOOTH) {
+        int maxkey = 0;
+        for (int y = 0; y < N; ++y)
+            for (int z = 0; z < N; ++z)
+                for (int x = 0; x < c->nxv; ++x) {
+                    const double kx = x * c->dkx, ky = kwrap_h(y, N, c->dky), kz = kwrap_h(z, N, c->dkz);
+                    const double k2 = (kx * kx + ky * ky) + kz * kz;
+                    maxkey = std::max(maxkey, (int)std::round(k2 / c->dk2));
+                }
+        filt.assign((size_t)maxkey + 1, 0.0);
+        for (int y = 0; y < N; ++y)
+            for (int z = 0; z < N; ++z)
+                for (int x = 0; x < c->nxv; ++x) {
+                    const double kx = x * c->dkx, ky = kwrap_h(y, N, c->dky), kz = kwrap_h(z, N, c->dkz);
+                    const double k2 = (kx * kx + ky * ky) + kz * kz;
+                    filt[(size_t)std::round(k2 / c->dk2)] = std::exp(-36.0 * std::pow(k2 / c->kM2, 18.));
+                }
+    } else {
+        filt.assign(1, 1.0);
+    }
+    c->nfilt = (int)filt.size();
+    const size_t tb = (size_t)c->real_bytes;
+    CU(cudaMalloc(&c->filt, filt.size() * tb));
+    if (c->real_bytes == 4) {
+        std::vector<float> f(filt.begin(), filt.end());
+        CU(cudaMemcpy(c->filt, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    } else {
+        CU(cudaMemcpy(c->filt, filt.data(), filt.size() * 8, cudaMemcpyHostToDevice));
+    }
+    // shells (kspace.cpp:109-150)
+    c->kshell.assign(c->nshells, 0.0);
+    c->nshell.assign(c->nshells, 0);
+    for (int y = 0; y < N; ++y)
+        for (int z = 0; z < N; ++z)
+            for (int x = 0; x < c->nxv; ++x) {
+                const double kx = x * c->dkx, ky = kwrap_h(y, N, c->dky), kz = kwrap_h(z, N, c->dkz);
+                const double k2 = (kx * kx + ky * ky) + kz * kz;
+                if (k2 < c->kM2) {
+                    const double kn = std::sqrt(k2);
+                    const int w = x == 0 ? 1 : 2;
+                    c->kshell[(int)(kn / c->dk)] += w * kn;
+                    c->nshell[(int)(kn / c->dk)] += w;
+                }
+            }
+    for (int s = 0; s < c->nshells; ++s)
+        if (c->nshell[s] != 0) c->kshell[s] /= c->nshell[s];
+    return 0;
+}
+
+// integrating-factor tables for (nu, dt), per axis
+static int ensure_factors(bfg_ctx* c, double dt) {
+    if (dt == c->fac_dt && c->nu == c->fac_nu) return 0;
+    const int N = c->n, nxv = c->nxv;
+    const int nf = nxv + 2 * N;
+    std::vector<double> f(3 * (size_t)nf);
+    const double mult[3] = {-dt, -dt / 2, dt / 2};
+    for (int k = 0; k < 3; ++k) {
+        for (int x = 0; x < nxv; ++x) {
+            const double kx = x * c->dkx;
+            f[k * nf + x] = std::exp(c->nu * kx * kx * mult[k]);
+        }
+        for (int y = 0; y < N; ++y) {
+            const double ky = kwrap_h(y, N, c->dky);
+            f[k * nf + nxv + y] = std::exp(c->nu * ky * ky * mult[k]);
+        }
+        for (int z = 0; z < N; ++z) {
+            const double kz = kwrap_h(z, N, c->dkz);
+            f[k * nf + nxv + N + z] = std::exp(c->nu * kz * kz * mult[k]);
+        }
+    }
+    if (c->real_bytes == 4) {
+        std::vector<float> g(f.begin(), f.end());
+        CU(cudaMemcpyAsync(c->fac, g.data(), g.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+    } else {
+        CU(cudaMemcpyAsync(c->fac, f.data(), f.size() * 8, cudaMemcpyHostToDevice, c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+    }
+    c->fac_dt = dt;
+    c->fac_nu = c->nu;
+    return 0;
+}
+
+static int ensure_ru(bfg_ctx* c) {
+    if (c->ru) return 0;
+    const size_t bytes = (size_t)c->n * c->n * c->n * 3 * c->real_bytes;
+    if (cudaMalloc(&c->ru, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, BFG_ENOMEM, "cannot allocate %zu bytes for the real velocity", bytes);
+    }
+    CU(cudaMemset(c->ru, 0, bytes));
+    return 0;
+}
+
+// ----------------------------------------------------------- tracers --
+template <typename T, int NB, int MM>
+static int launch_tracers(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out) {
+    const unsigned blocks = (unsigned)((p->n + 127) / 128);
+    if (blocks == 0) return 0;
+    Prof pr(c, K_TRACER);
+    tracer_kernel<T, NB, MM><<<blocks, 128, 0, c->stream>>>(pp, (const T*)c->ru, p->pos, p->hist,
+                                                           out);
+    return after_launch(c, "tracer_kernel");
+}
+
+template <typename T>
+static int tracers_dispatch(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out) {
+#define BFG_TR(NBv, MMv) \
+    if (p->neighbours == NBv && p->smoothness == MMv) return launch_tracers<T, NBv, MMv>(c, pp, p, out);
+    BFG_TR(1, 0) BFG_TR(1, 1) BFG_TR(1, 2)
+    BFG_TR(2, 0) BFG_TR(2, 1) BFG_TR(2, 2)
+    BFG_TR(3, 0) BFG_TR(3, 1) BFG_TR(3, 2)
+    BFG_TR(4, 0) BFG_TR(4, 1) BFG_TR(4, 2)
+    BFG_TR(5, 0) BFG_TR(5, 1) BFG_TR(5, 2)
+#undef BFG_TR
+    return fail(c, BFG_EUNSUP, "interpolation (%d, %d) not supported", p->neighbours, p->smoothness);
+}
+
+static PParams pparams(const bfg_pctx* p, double dt, int move) {
+    const bfg_ctx* c = p->ctx;
+    PParams pp;
+    pp.n = p->n;
+    pp.N = c->n;
+    const double dks[3] = {c->dkx, c->dky, c->dkz};
+    for (int d = 0; d < 3; ++d) {
+        pp.box[d] = 4 * std::acos(0.0) / dks[d];
+        pp.hstep[d] = pp.box[d] / (double)c->n;
+    }
+    pp.nsteps = p->nsteps;
+    pp.head = p->head;
+    pp.order = std::min(p->step_idx, p->nsteps);
+    pp.accum = p->rhs0_zero ? 0 : 1;
+    pp.move = move;
+    pp.dt = dt;
+    return pp;
+}
+
+static int tracer_loop(bfg_pctx* p, double dt) {
+    bfg_ctx* c = p->ctx;
+    if (p->step_idx > 6 && p->nsteps > 6)
+        return fail(c, BFG_EINVAL, "Adams-Bashforth order above 6");
+    PParams pp = pparams(p, dt, 1);
+    int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, nullptr)
+                                : tracers_dispatch<double>(c, pp, p, nullptr);
+    if (rc) return rc;
+    // inc_step_idx, shift_rhs_vectors
+    p->step_idx += 1;
+    p->head = (p->head - 1 + p->nsteps) % p->nsteps;
+    p->rhs0_zero = true;
+    return 0;
+}
+
+template <typename T, int N>
+int OpStep<T, N>::run(bfg_ctx* c, double dt, bfg_pctx* p) {
+    int rc;
+    if ((rc = Engine<T, N>::stage(c, 0, dt, p != nullptr))) return rc;
+    if (p && (rc = tracer_loop(p, dt))) return rc;
+    if ((rc = Engine<T, N>::stage(c, 1, dt, false))) return rc;
+    if ((rc = Engine<T, N>::stage(c, 2, dt, false))) return rc;
+    return Engine<T, N>::finish_step(c);
+}
+
+// ================================================================ ABI ==
+extern "C" {
+
+const char* bfg_version(void) { return BFG_VERSION; }
+
+const char* bfg_last_error(const bfg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void bfg_ctx_destroy(bfg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* bufs[] = {c->w0, c->v1, c->v2, c->wa, c->wb, c->ru, c->tw, c->filt, c->fac, c->stats_ws};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int bfg_ctx_create(bfg_ctx** out, int nx, int ny, int nz, double dkx, double dky, double dkz,
+                   int real_bytes, int dealias_type, int device) {
+    if (!out) return BFG_EINVAL;
+    *out = nullptr;
+    if (nx != ny || nx != nz) return BFG_EUNSUP;
+    if (!is_pow2(nx) || nx < 16 || nx > 1024) return BFG_EUNSUP;
+    if (real_bytes != 4 && real_bytes != 8) return BFG_EINVAL;
+    if (dealias_type != BFG_SMOOTH && dealias_type != BFG_TWO_THIRDS) return BFG_EINVAL;
+    if (!(dkx > 0 && dky > 0 && dkz > 0)) return BFG_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return BFG_ECUDA;
+    }
+    if (device < 0 || device >= ndev) return BFG_EINVAL;
+    bfg_ctx* c = new bfg_ctx();
+    c->n = nx;
+    c->nxv = nx / 2 + 1;
+    c->nxp = nx / 2 + 4;
+    c->real_bytes = real_bytes;
+    c->dealias = dealias_type;
+    c->device = device;
+    c->dkx = dkx;
+    c->dky = dky;
+    c->dkz = dkz;
+    // kspace.cpp:75-100 (cubic grid: sizes are (n, n, n/2+1))
+    const int s0 = nx, s1 = nx, s2 = nx / 2 + 1;
+    double kMx, kMy, kMz;
+    if (dealias_type == BFG_TWO_THIRDS) {
+        kMx = dkx * ((2 * (s2 - 1)) / 3 - 1);
+        kMy = dky * (s0 / 3 - 1);
+        kMz = dkz * (s1 / 3 - 1);
+    } else {
+        kMx = dkx * (s2 - 2);
+        kMy = dky * (s0 / 2 - 1);
+        kMz = dkz * (s1 / 2 - 1);
+    }
+    c->kM = std::max(kMx, std::max(kMy, kMz));
+    c->kM2 = c->kM * c->kM;
+    c->dk = std::min(dkx, std::min(dky, dkz));
+    c->dk2 = c->dk * c->dk;
+    c->nshells = (int)(c->kM / c->dk) + 2;
+    int rc = 0;
+    auto bail = [&](int code) {
+        bfg_ctx_destroy(c);
+        return code;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(BFG_ECUDA);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(BFG_ECUDA);
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+    const size_t cb = 2 * (size_t)real_bytes;  // bytes per complex
+    c->field_bytes = (size_t)nx * nx * c->nxp * 3 * cb;
+    void** bufs[] = {&c->w0, &c->v1, &c->v2, &c->wa, &c->wb};
+    for (void** b : bufs) {
+        if (cudaMalloc(b, c->field_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(BFG_ENOMEM);
+        }
+        if (cudaMemset(*b, 0, c->field_bytes) != cudaSuccess) return bail(BFG_ECUDA);
+    }
+    if (cudaMalloc(&c->tw, (size_t)nx * cb) != cudaSuccess) return bail(BFG_ENOMEM);
+    if (cudaMalloc(&c->fac, 3 * (size_t)(c->nxv + 2 * nx) * real_bytes) != cudaSuccess)
+        return bail(BFG_ENOMEM);
+    if ((rc = upload_tables(c))) return bail(rc);
+    *out = c;
+    return BFG_OK;
+}
+
+int bfg_set_physics(bfg_ctx* c, double nu, int forcing_type, double famplitude, double fk0,
+                    double fk1, int fmode) {
+    if (!c) return BFG_EINVAL;
+    if (forcing_type < BFG_FORCING_NONE || forcing_type > BFG_FORCING_KOLMOGOROV)
+        return fail(c, BFG_EINVAL, "unknown forcing_type %d", forcing_type);
+    if (forcing_type == BFG_FORCING_KOLMOGOROV && (fmode < 0 || fmode >= c->n))
+        return fail(c, BFG_EINVAL, "fmode %d outside the grid", fmode);
+    c->nu = nu;
+    c->forcing = forcing_type;
+    c->famp = famplitude;
+    c->fk0 = fk0;
+    c->fk1 = fk1;
+    c->fmode = fmode;
+    return 0;
+}
+
+int bfg_kspace_info(const bfg_ctx* c, double* kM, double* dk, int* nshells, double* kshell,
+                    int64_t* nshell) {
+    if (!c) return BFG_EINVAL;
+    if (kM) *kM = c->kM;
+    if (dk) *dk = c->dk;
+    if (nshells) *nshells = c->nshells;
+    if (kshell) std::copy(c->kshell.begin(), c->kshell.end(), kshell);
+    if (nshell) std::copy(c->nshell.begin(), c->nshell.end(), nshell);
+    return 0;
+}
+
+static int field_copy(bfg_ctx* c, int field_id, void* host, bool upload) {
+    if (!c || !host) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    const size_t cb = 2 * (size_t)c->real_bytes;
+    const size_t N = c->n;
+    if (field_id == BFG_FIELD_VORTICITY || field_id == BFG_FIELD_VELOCITY) {
+        void* dev = field_id == BFG_FIELD_VORTICITY ? c->w0 : c->wa;
+        const size_t dpitch = (size_t)c->nxp * 3 * cb, hpitch = (size_t)c->nxv * 3 * cb;
+        if (upload)
+            CU(cudaMemcpy2DAsync(dev, dpitch, host, hpitch, hpitch, N * N, cudaMemcpyHostToDevice,
+                                 c->stream));
+        else
+            CU(cudaMemcpy2DAsync(host, hpitch, dev, dpitch, hpitch, N * N, cudaMemcpyDeviceToHost,
+                                 c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+        return 0;
+    }
+    if (field_id == BFG_FIELD_RVELOCITY) {
+        int rc = ensure_ru(c);
+        if (rc) return rc;
+        const size_t rb = c->real_bytes;
+        const size_t dpitch = N * 3 * rb, hpitch = (N + 2) * 3 * rb;
+        if (upload) {
+            CU(cudaMemcpy2DAsync(c->ru, dpitch, host, hpitch, dpitch, N * N, cudaMemcpyHostToDevice,
+                                 c->stream));
+        } else {
+            CU(cudaMemcpy2DAsync(host, hpitch, c->ru, dpitch, dpitch, N * N, cudaMemcpyDeviceToHost,
+                                 c->stream));
+        }
+        CU(cudaStreamSynchronize(c->stream));
+        if (!upload) {
+            for (size_t r = 0; r < N * N; ++r)
+                memset((char*)host + r * hpitch + dpitch, 0, hpitch - dpitch);
+        }
+        return 0;
+    }
+    return fail(c, BFG_EINVAL, "unknown field id %d", field_id);
+}
+
+int bfg_field_upload(bfg_ctx* c, int field_id, const void* host) {
+    return field_copy(c, field_id, const_cast<void*>(host), true);
+}
+int bfg_field_download(bfg_ctx* c, int field_id, void* host) {
+    return field_copy(c, field_id, host, false);
+}
+
+int bfg_read_checkpoint_fixup(bfg_ctx* c) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    int rc = dispatch<OpFixup>(c);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_nsveparticles_step(bfg_ctx* c, bfg_pctx* p, double dt, int nsteps) {
+    if (!c || nsteps < 0) return BFG_EINVAL;
+    if (p && p->ctx != c) return fail(c, BFG_EINVAL, "tracers belong to another context");
+    CU(cudaSetDevice(c->device));
+    int rc = ensure_factors(c, dt);
+    if (rc) return rc;
+    if (p && (rc = ensure_ru(c))) return rc;
+    CU(cudaEventRecord(c->ev0, c->stream));
+    for (int s = 0; s < nsteps; ++s) {
+        if ((rc = dispatch<OpStep>(c, dt, p))) return rc;
+        c->iteration++;
+    }
+    CU(cudaEventRecord(c->ev1, c->stream));
+    return 0;
+}
+
+int bfg_step(bfg_ctx* c, double dt, int nsteps) { return bfg_nsveparticles_step(c, nullptr, dt, nsteps); }
+
+int bfg_compute_velocity(bfg_ctx* c) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    int rc = dispatch<OpVelocity>(c);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_velocity_rspace(bfg_ctx* c) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    rc = dispatch<OpVelocityR>(c);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
+    if (!c || !din || !dout) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
+    CU(cudaMemcpy2DAsync(c->wb, c->nxp * 3 * cb, din, c->nxv * 3 * cb, c->nxv * 3 * cb, N * N,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = dispatch<OpIft>(c))) return rc;
+    CU(cudaMemset2DAsync(dout, (N + 2) * 3 * rb, 0, (N + 2) * 3 * rb, N * N, c->stream));
+    CU(cudaMemcpy2DAsync(dout, (N + 2) * 3 * rb, c->ru, N * 3 * rb, N * 3 * rb, N * N,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_dft(bfg_ctx* c, const void* din, void* dout) {
+    if (!c || !din || !dout) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
+    CU(cudaMemcpy2DAsync(c->ru, N * 3 * rb, din, (N + 2) * 3 * rb, N * 3 * rb, N * N,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = dispatch<OpDft>(c))) return rc;
+    CU(cudaMemcpy2DAsync(dout, c->nxv * 3 * cb, c->wb, c->nxp * 3 * cb, c->nxv * 3 * cb, N * N,
+                         cudaMemcpyDeviceToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_get_iteration(const bfg_ctx* c, int* it) {
+    if (!c || !it) return BFG_EINVAL;
+    *it = c->iteration;
+    return 0;
+}
+int bfg_set_iteration(bfg_ctx* c, int it) {
+    if (!c) return BFG_EINVAL;
+    c->iteration = it;
+    return 0;
+}
+
+int bfg_last_step_ms(bfg_ctx* c, double* ms) {
+    if (!c || !ms) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    CU(cudaEventSynchronize(c->ev1));
+    float f = 0;
+    CU(cudaEventElapsedTime(&f, c->ev0, c->ev1));
+    *ms = f;
+    return 0;
+}
+
+int bfg_profile(bfg_ctx* c, int enable) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    prof_flush(c);
+    c->prof = enable != 0;
+    if (enable)
+        for (int k = 0; k < BFG_NKINDS; ++k) {
+            c->prof_ms[k] = 0;
+            c->prof_n[k] = 0;
+        }
+    return 0;
+}
+
+int bfg_profile_read(bfg_ctx* c, int kind, double* total_ms, int64_t* launches) {
+    if (!c || kind < 0 || kind >= BFG_NKINDS) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    prof_flush(c);
+    if (total_ms) *total_ms = c->prof_ms[kind];
+    if (launches) *launches = c->prof_n[kind];
+    return 0;
+}
+
+int bfg_kernel_launches(const bfg_ctx* c, int64_t* count) {
+    if (!c || !count) return BFG_EINVAL;
+    *count = c->launches;
+    return 0;
+}
+
+int bfg_stats(bfg_ctx* c, double max_velocity_estimate, double max_vorticity_estimate, int nbins,
+              double* spec_vel, double* spec_vort, double* mom_vel, double* mom_vort,
+              int64_t* hist_vel, int64_t* hist_vort) {
+    if (!c || nbins <= 0) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    // vorticity: state itself; velocity: compute_velocity(cvorticity)
+    if ((rc = dispatch<OpStats>(c, (const void*)c->w0, max_vorticity_estimate / std::sqrt(3.0),
+                                nbins, spec_vort, mom_vort, hist_vort)))
+        return rc;
+    if ((rc = dispatch<OpVelocity>(c))) return rc;
+    if ((rc = dispatch<OpStats>(c, (const void*)c->wa, max_velocity_estimate / std::sqrt(3.0),
+                                nbins, spec_vel, mom_vel, hist_vel)))
+        return rc;
+    return 0;
+}
+
+// ------------------------------------------------------------ tracers --
+int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, int smoothness,
+                         int nsteps, const double* pos, const double* rhs, const int64_t* idx,
+                         int step_idx) {
+    if (!c || !out || n < 0 || (n > 0 && !pos)) return BFG_EINVAL;
+    *out = nullptr;
+    if (neighbours < 1 || neighbours > 5 || smoothness < 0 || smoothness > 2)
+        return fail(c, BFG_EUNSUP, "interpolation (%d, %d) not supported", neighbours, smoothness);
+    if (nsteps < 1 || nsteps > 6)
+        return fail(c, BFG_EINVAL, "nsteps %d outside 1..6 (particles_adams_bashforth.hpp:24-28)",
+                    nsteps);
+    if (step_idx < 1) return fail(c, BFG_EINVAL, "step_idx must be >= 1");
+    CU(cudaSetDevice(c->device));
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    bfg_pctx* p = new bfg_pctx();
+    p->ctx = c;
+    p->n = n;
+    p->neighbours = neighbours;
+    p->smoothness = smoothness;
+    p->nsteps = nsteps;
+    p->step_idx = step_idx;
+    p->head = 0;
+    const size_t nb = (size_t)std::max<int64_t>(n, 1) * 3 * sizeof(double);
+    if (cudaMalloc(&p->pos, nb) != cudaSuccess || cudaMalloc(&p->hist, nb * nsteps) != cudaSuccess ||
+        cudaMalloc(&p->sample, nb) != cudaSuccess) {
+        cudaGetLastError();
+        bfg_particles_destroy(p);
+        return fail(c, BFG_ENOMEM, "cannot allocate tracer state for %lld tracers", (long long)n);
+    }
+    auto cleanup = [&](int code) {
+        bfg_particles_destroy(p);
+        return code;
+    };
+    if (n > 0) {
+        if (cudaMemcpy(p->pos, pos, (size_t)n * 3 * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+            return cleanup(fail(c, BFG_ECUDA, "tracer upload failed"));
+        if (rhs) {
+            if (cudaMemcpy(p->hist, rhs, (size_t)n * 3 * 8 * nsteps, cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+                return cleanup(fail(c, BFG_ECUDA, "tracer upload failed"));
+            bool z = true;
+            for (int64_t i = 0; i < n * 3 && z; ++i) z = rhs[i] == 0.0;
+            p->rhs0_zero = z;
+        } else {
+            cudaMemset(p->hist, 0, (size_t)n * 3 * 8 * nsteps);
+            p->rhs0_zero = true;
+        }
+    }
+    p->idx.resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) p->idx[i] = idx ? idx[i] : i;
+    *out = p;
+    return 0;
+}
+
+void bfg_particles_destroy(bfg_pctx* p) {
+    if (!p) return;
+    if (p->ctx) cudaSetDevice(p->ctx->device);
+    if (p->pos) cudaFree(p->pos);
+    if (p->hist) cudaFree(p->hist);
+    if (p->sample) cudaFree(p->sample);
+    delete p;
+}
+
+int bfg_particles_complete_loop(bfg_pctx* p, double dt) {
+    if (!p) return BFG_EINVAL;
+    bfg_ctx* c = p->ctx;
+    CU(cudaSetDevice(c->device));
+    int rc = tracer_loop(p, dt);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+static int to_index_order(bfg_pctx* p, const std::vector<double>& dev_order, int width,
+                          double* out) {
+    // tracers are kept in creation order; the reference writes them sorted by
+    // global index (abstract_particles_output.hpp:144-265)
+    std::vector<int64_t> order(p->n);
+    for (int64_t i = 0; i < p->n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(),
+              [&](int64_t a, int64_t b) { return p->idx[a] < p->idx[b]; });
+    for (int64_t k = 0; k < p->n; ++k)
+        for (int d = 0; d < width; ++d) out[k * width + d] = dev_order[order[k] * width + d];
+    return 0;
+}
+
+int bfg_particles_sample_velocity(bfg_pctx* p, double* out) {
+    if (!p || !out) return BFG_EINVAL;
+    bfg_ctx* c = p->ctx;
+    CU(cudaSetDevice(c->device));
+    PParams pp = pparams(p, 0.0, 0);
+    int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, p->sample)
+                                : tracers_dispatch<double>(c, pp, p, p->sample);
+    if (rc) return rc;
+    std::vector<double> h((size_t)p->n * 3);
+    CU(cudaMemcpyAsync(h.data(), p->sample, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return to_index_order(p, h, 3, out);
+}
+
+int bfg_particles_download(bfg_pctx* p, double* pos, double* rhs, int64_t* idx) {
+    if (!p) return BFG_EINVAL;
+    bfg_ctx* c = p->ctx;
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    const size_t n3 = (size_t)p->n * 3;
+    if (pos) {
+        std::vector<double> h(n3);
+        CU(cudaMemcpy(h.data(), p->pos, n3 * 8, cudaMemcpyDeviceToHost));
+        to_index_order(p, h, 3, pos);
+    }
+    if (rhs) {
+        std::vector<double> h(n3);
+        for (int j = 0; j < p->nsteps; ++j) {
+            if (j == 0 && p->rhs0_zero) {
+                std::fill(rhs, rhs + n3, 0.0);
+                continue;
+            }
+            const int slot = (p->head + j) % p->nsteps;
+            CU(cudaMemcpy(h.data(), p->hist + (size_t)slot * n3, n3 * 8, cudaMemcpyDeviceToHost));
+            to_index_order(p, h, 3, rhs + (size_t)j * n3);
+        }
+    }
+    if (idx) {
+        std::vector<int64_t> s(p->idx);
+        std::sort(s.begin(), s.end());
+        std::copy(s.begin(), s.end(), idx);
+    }
+    return 0;
+}
+
+int bfg_particles_upload(bfg_pctx* p, const double* pos, const double* rhs, int step_idx) {
+    if (!p || (p->n > 0 && !pos) || step_idx < 1) return BFG_EINVAL;
+    bfg_ctx* c = p->ctx;
+    CU(cudaSetDevice(c->device));
+    const size_t n3 = (size_t)p->n * 3;
+    CU(cudaMemcpyAsync(p->pos, pos, n3 * 8, cudaMemcpyHostToDevice, c->stream));
+    p->head = 0;
+    if (rhs) {
+        CU(cudaMemcpyAsync(p->hist, rhs, n3 * 8 * p->nsteps, cudaMemcpyHostToDevice, c->stream));
+        bool z = true;
+        for (size_t i = 0; i < n3 && z; ++i) z = rhs[i] == 0.0;
+        p->rhs0_zero = z;
+    } else {
+        CU(cudaMemsetAsync(p->hist, 0, n3 * 8 * p->nsteps, c->stream));
+        p->rhs0_zero = true;
+    }
+    p->step_idx = step_idx;
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_particles_info(const bfg_pctx* p, int64_t* n, int* nsteps, int* step_idx) {
+    if (!p) return BFG_EINVAL;
+    if (n) *n = p->n;
+    if (nsteps) *nsteps = p->nsteps;
+    if (step_idx) *step_idx = p->step_idx;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,242 @@
+// Shared-memory FFT building blocks for the sm_100a NSVE kernels.
+//
+// All transforms here are power-of-two, in place, on "pencils" that live in
+// shared memory.  A pencil of length L is addressed as
+//     s[p * PS + e * ES]      (pencil p, element e)
+// so the same code serves the strided-axis passes (pencils side by side,
+// ES = row pitch, PS = 1) and the row pass (pencils contiguous, ES = 1).
+//
+// Two in-place forms are used:
+//   * DIF (Gentleman-Sande): natural-order input, digit-reversed output;
+//   * DIT (Cooley-Tukey):    digit-reversed input, natural-order output.
+// The digit order of a length-L transform with stage radices R1, R2, ... is
+//   position(k) = q1*(L/R1) + q2*(L/(R1*R2)) + ...,  k = q1 + R1*(q2 + R2*(...)).
+// Radices are 8, then 4 or 2 for the remainder (plan_step below).
+//
+// Twiddles come from one table tw[m] = exp(-2*pi*i*m/TAB), m < TAB, built on
+// the host in long double and rounded once to the working precision; any
+// transform length L dividing TAB indexes it with stride TAB/L.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bfg {
+
+template <typename T>
+struct __align__(2 * sizeof(T)) cpx {
+    T x, y;
+};
+
+template <typename T>
+__device__ __forceinline__ cpx<T> mk(T a, T b) {
+    cpx<T> r;
+    r.x = a;
+    r.y = b;
+    return r;
+}
+template <typename T>
+__device__ __forceinline__ cpx<T> operator+(cpx<T> a, cpx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
+template <typename T>
+__device__ __forceinline__ cpx<T> operator-(cpx<T> a, cpx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+template <typename T>
+__device__ __forceinline__ cpx<T> cmul(cpx<T> a, cpx<T> b) {
+    return mk<T>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename T>
+__device__ __forceinline__ cpx<T> cmulc(cpx<T> a, cpx<T> b) {  // a * conj(b)
+    return mk<T>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename T>
+__device__ __forceinline__ cpx<T> conjg(cpx<T> a) { return mk<T>(a.x, -a.y); }
+template <typename T>
+__device__ __forceinline__ cpx<T> scale(cpx<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
+// multiply by -i (forward sign) or +i (inverse sign)
+template <typename T, bool INV>
+__device__ __forceinline__ cpx<T> rot90(cpx<T> a) {
+    return INV ? mk<T>(-a.y, a.x) : mk<T>(a.y, -a.x);
+}
+
+// ---------------------------------------------------------------- plans --
+__host__ __device__ constexpr int plan_step(int L) {
+    return (L % 8 == 0 && L / 8 != 2) ? 8 : ((L % 4 == 0) ? 4 : 2);
+}
+__host__ __device__ constexpr int plan_nstages(int L) {
+    return L <= 1 ? 0 : 1 + plan_nstages(L / plan_step(L));
+}
+// radix of stage s
+__host__ __device__ constexpr int plan_radix(int L, int s) {
+    return s == 0 ? plan_step(L) : plan_radix(L / plan_step(L), s - 1);
+}
+// block length at stage s (L at s = 0, divided by the earlier radices)
+__host__ __device__ constexpr int plan_block(int L, int s) {
+    return s == 0 ? L : plan_block(L / plan_step(L), s - 1);
+}
+
+// position of frequency k after a DIF of length L
+template <int L>
+__device__ __forceinline__ int dif_position(int k) {
+    int pos = 0;
+    int rem = k;
+    int Lr = L;
+#pragma unroll
+    for (int s = 0; s < plan_nstages(L); ++s) {
+        const int R = plan_step(Lr);
+        const int q = rem % R;
+        rem /= R;
+        Lr /= R;
+        pos += q * Lr;
+    }
+    return pos;
+}
+
+// ------------------------------------------------------- small DFTs --
+template <typename T, bool INV>
+__device__ __forceinline__ void dft2(cpx<T>* v) {
+    cpx<T> t = v[0] - v[1];
+    v[0] = v[0] + v[1];
+    v[1] = t;
+}
+template <typename T, bool INV>
+__device__ __forceinline__ void dft4(cpx<T>* v) {
+    cpx<T> s02 = v[0] + v[2], d02 = v[0] - v[2];
+    cpx<T> s13 = v[1] + v[3], d13 = rot90<T, INV>(v[1] - v[3]);
+    v[0] = s02 + s13;
+    v[2] = s02 - s13;
+    v[1] = d02 + d13;
+    v[3] = d02 - d13;
+}
+template <typename T, bool INV>
+__device__ __forceinline__ void dft8(cpx<T>* v) {
+    cpx<T> e[4] = {v[0], v[2], v[4], v[6]};
+    cpx<T> o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<T, INV>(e);
+    dft4<T, INV>(o);
+    const T h = (T)0.70710678118654752440084436210484903928;  // 1/sqrt(2)
+    // o[q] *= exp(-+ 2 pi i q / 8)
+    o[1] = INV ? mk<T>(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+               : mk<T>(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    o[2] = rot90<T, INV>(o[2]);
+    o[3] = INV ? mk<T>(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+               : mk<T>(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        v[q] = e[q] + o[q];
+        v[q + 4] = e[q] - o[q];
+    }
+}
+template <typename T, bool INV, int R>
+__device__ __forceinline__ void dft(cpx<T>* v) {
+    if constexpr (R == 2) dft2<T, INV>(v);
+    else if constexpr (R == 4) dft4<T, INV>(v);
+    else dft8<T, INV>(v);
+}
+
+template <typename T, bool INV>
+__device__ __forceinline__ cpx<T> twiddle(const cpx<T>* tw, int idx) {
+    cpx<T> t = tw[idx];
+    if (INV) t.y = -t.y;
+    return t;
+}
+
+// ----------------------------------------------------------- stages --
+// One DIF stage S of a length-L transform over P pencils.
+// PFAST: consecutive threads take consecutive pencils (pencils adjacent in
+// shared memory); otherwise consecutive threads take consecutive elements.
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+__device__ __forceinline__ void dif_stage(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    constexpr int R = plan_radix(L, S);
+    constexpr int Ls = plan_block(L, S);
+    constexpr int span = Ls / R;
+    constexpr int NBLK = L / Ls;
+    constexpr int NW = P * NBLK * span;
+    for (int w = tid; w < NW; w += nthr) {
+        int p, b, j;
+        if (PFAST) {
+            p = w % P;
+            const int r = w / P;
+            j = r % span;
+            b = r / span;
+        } else {
+            j = w % span;
+            const int r = w / span;
+            b = r % NBLK;
+            p = r / NBLK;
+        }
+        const int base = p * PS + (b * Ls + j) * ES;
+        cpx<T> v[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[m] = s[base + m * span * ES];
+        dft<T, INV, R>(v);
+        if (span > 1) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], twiddle<T, INV>(tw, j * q * (TAB / Ls)));
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) s[base + q * span * ES] = v[q];
+    }
+}
+
+// One DIT stage S (stages run from the last DIF stage back to stage 0).
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+__device__ __forceinline__ void dit_stage(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    constexpr int R = plan_radix(L, S);
+    constexpr int Ls = plan_block(L, S);
+    constexpr int span = Ls / R;
+    constexpr int NBLK = L / Ls;
+    constexpr int NW = P * NBLK * span;
+    for (int w = tid; w < NW; w += nthr) {
+        int p, b, j;
+        if (PFAST) {
+            p = w % P;
+            const int r = w / P;
+            j = r % span;
+            b = r / span;
+        } else {
+            j = w % span;
+            const int r = w / span;
+            b = r % NBLK;
+            p = r / NBLK;
+        }
+        const int base = p * PS + (b * Ls + j) * ES;
+        cpx<T> v[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[m] = s[base + m * span * ES];
+        if (span > 1) {
+#pragma unroll
+            for (int m = 1; m < R; ++m) v[m] = cmul(v[m], twiddle<T, INV>(tw, j * m * (TAB / Ls)));
+        }
+        dft<T, INV, R>(v);
+#pragma unroll
+        for (int q = 0; q < R; ++q) s[base + q * span * ES] = v[q];
+    }
+}
+
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+__device__ __forceinline__ void dif_from(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    if constexpr (S < plan_nstages(L)) {
+        dif_stage<T, L, S, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+        __syncthreads();
+        dif_from<T, L, S + 1, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+    }
+}
+// Full DIF transform: natural in, digit-reversed out.  Ends with a barrier.
+template <typename T, int L, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+__device__ __forceinline__ void dif(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    dif_from<T, L, 0, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+}
+
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+__device__ __forceinline__ void dit_down(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    if constexpr (S >= 0) {
+        dit_stage<T, L, S, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+        __syncthreads();
+        dit_down<T, L, S - 1, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+    }
+}
+// Full DIT transform: digit-reversed in, natural out.  Ends with a barrier.
+template <typename T, int L, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+__device__ __forceinline__ void dit(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    dit_down<T, L, plan_nstages(L) - 1, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+}
+
+}  // namespace bfg

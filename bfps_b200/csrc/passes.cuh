@@ -1,0 +1,576 @@
+// Fused HBM passes of the IF-RK3 vorticity step (sm_100a).
+//
+// Device layouts (units of "points" = 3 complex numbers, one per component):
+//   state  S: [ky][kz][kx]  point (ky*N + kz)*NXP + kx   (reference layout,
+//                                                       rows padded to NXP)
+//   work   W: [z][y][kx]    point (z*N + y)*NXP + kx     (after z / y passes)
+//   real   R: [z][y][x][c]  scalar ((z*N + y)*N + x)*3 + c (unpadded)
+// kx runs over NXV = N/2+1 valid columns; NXP = N/2+4 keeps every row
+// 32-byte aligned.
+//
+// One RK stage is five launches:
+//   IZ  (col pass, a=ky, FFT over kz)  S -> W : u^ = i k x w^ / k^2 (+ w^)
+//   IY  (col pass, a=z,  FFT over ky)  W -> W
+//   X   (row pass, one (z,y) row)      W -> W : C2R of u, w; u x w / N^3;
+//                                               R2C of the product
+//   FY  (col pass, a=z,  FFT over y)   W -> W
+//   FZ  (col pass, a=ky, FFT over z)   W -> S : dealias, i k x, forcing,
+//                                               force_divfree, RK update
+// Reference: vorticity_equation.cpp:206-239 (compute_velocity), :290-356
+// (omega_nonlin), :358-439 (step); kspace.cpp:461-519 (dealias,
+// force_divfree).
+#pragma once
+#include "fft.cuh"
+
+namespace bfg {
+
+struct KParams {
+    int nxv;           // N/2 + 1
+    int nxp;           // padded row length (points)
+    double dkx, dky, dkz;
+    double kM2;
+    int dealias;       // 0 two-thirds, 1 smooth
+    double inv_dk2;    // 1 / dk^2 (smooth filter key)
+    int nfilt;         // filter table length
+    int forcing;       // 0 none, 1 linear, 2 Kolmogorov
+    double famp, fk0, fk1;
+    int fmode;
+    double dt;
+};
+
+enum ColMode {
+    CM_IZ_VEL = 0,    // S -> (u^, w^) in W
+    CM_IZ_PLAIN = 1,  // S -> W (inverse over kz)
+    CM_Y_INV2 = 2,    // W, W in place (inverse over ky)
+    CM_Y_INV1 = 3,
+    CM_Y_FWD1 = 4,    // W in place (forward over y)
+    CM_FZ_RK1 = 5,    // W -> S with the stage-1 update
+    CM_FZ_RK2 = 6,
+    CM_FZ_RK3 = 7,
+    CM_FZ_PLAIN = 8,  // W -> S (forward over z)
+    CM_IZ_U = 9,      // S -> u^ in W (inverse over kz of compute_velocity)
+};
+
+__host__ __device__ constexpr int col_nb(int mode) {
+    return (mode == CM_IZ_VEL || mode == CM_Y_INV2) ? 2 : 1;
+}
+__host__ __device__ constexpr int col_nbin(int mode) { return mode == CM_Y_INV2 ? 2 : 1; }
+__host__ __device__ constexpr bool col_inverse(int mode) {
+    return mode <= CM_Y_INV1 || mode == CM_IZ_U;
+}
+__host__ __device__ constexpr int pow2floor(int v) {
+    return v < 2 ? 1 : 2 * pow2floor(v / 2);
+}
+// kx columns per CTA: keep the tile near 96 KB (two CTAs per SM)
+template <typename T, int N, int NB>
+__host__ __device__ constexpr int col_tkx() {
+    return pow2floor(98304 / (N * NB * 3 * (int)sizeof(cpx<T>))) > 16
+               ? 16
+               : pow2floor(98304 / (N * NB * 3 * (int)sizeof(cpx<T>)));
+}
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr int col_pitch() {  // complex per tile row
+    return col_nb(MODE) * 3 * col_tkx<T, N, col_nb(MODE)>() + 1;
+}
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr size_t col_smem_bytes() {
+    return (size_t)(N * col_pitch<T, N, MODE>() + N) * sizeof(cpx<T>);
+}
+constexpr int COL_THREADS = 256;
+
+template <int N>
+__device__ __forceinline__ double kwrap(int i, double dk) {
+    return dk * (double)(i <= N / 2 ? i : i - N);
+}
+
+// i k x a  (vorticity_equation.cpp:323-336)
+template <typename A>
+__device__ __forceinline__ void curl(A kx, A ky, A kz, const cpx<A>* a, cpx<A>* t) {
+    t[0] = mk<A>(-(ky * a[2].y - kz * a[1].y), (ky * a[2].x - kz * a[1].x));
+    t[1] = mk<A>(-(kz * a[0].y - kx * a[2].y), (kz * a[0].x - kx * a[2].x));
+    t[2] = mk<A>(-(kx * a[1].y - ky * a[0].y), (kx * a[1].x - ky * a[0].x));
+}
+
+// kspace::force_divfree on one mode (kspace.cpp:487-519), k2 > 0
+template <typename A>
+__device__ __forceinline__ void divfree(A kx, A ky, A kz, A inv_k2, cpx<A>* a) {
+    const A tr = (kx * a[0].x + ky * a[1].x + kz * a[2].x) * inv_k2;
+    const A ti = (kx * a[0].y + ky * a[1].y + kz * a[2].y) * inv_k2;
+    a[0].x -= tr * kx; a[0].y -= ti * kx;
+    a[1].x -= tr * ky; a[1].y -= ti * ky;
+    a[2].x -= tr * kz; a[2].y -= ti * kz;
+}
+
+template <typename T>
+__device__ __forceinline__ cpx<T> zero_c() { return mk<T>((T)0, (T)0); }
+
+// ---------------------------------------------------------------------------
+// Strided-axis pass.  grid = (kx tiles, N): blockIdx.y is the fixed outer
+// index a, the transform runs along l over N rows of the tile.
+// fac: per-axis integrating-factor tables, 3 factors x (NXV + N + N):
+//      [f][0..NXV) kx, [f][NXV..NXV+N) ky, [f][NXV+N..NXV+2N) kz, where
+//      f = 0: exp(-nu k^2 dt), 1: exp(-nu k^2 dt/2), 2: exp(+nu k^2 dt/2)
+//      per axis (their product over the axes is the factor of k^2).
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(COL_THREADS)
+col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restrict__ in1,
+         cpx<T>* out0, cpx<T>* out1, const cpx<T>* __restrict__ rk_v0,
+         const cpx<T>* __restrict__ rk_vp, const cpx<T>* __restrict__ fsrc,
+         const T* __restrict__ filt, const T* __restrict__ fac,
+         const cpx<T>* __restrict__ tw_g) {
+    constexpr int NB = col_nb(MODE);
+    constexpr int NBIN = col_nbin(MODE);
+    constexpr int TKX = col_tkx<T, N, NB>();
+    constexpr int W = 3 * TKX;                     // complex per row per buffer
+    constexpr int PR = col_pitch<T, N, MODE>();    // tile row pitch
+    constexpr bool INV = col_inverse(MODE);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* tile = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* tw = tile + N * PR;
+
+    const int tid = threadIdx.x;
+    const int a = blockIdx.y;
+    const int kx0 = blockIdx.x * TKX;
+    const int ncol = min(TKX, kp.nxv - kx0);
+    const size_t nxp3 = (size_t)kp.nxp * 3;
+
+    for (int i = tid; i < N; i += COL_THREADS) tw[i] = tw_g[i];
+
+    // ---- load (rows l, buffers b, complex q) ---------------------------
+    for (int e = tid; e < N * NBIN * W; e += COL_THREADS) {
+        const int q = e % W;
+        const int r = e / W;
+        const int b = r % NBIN;
+        const int l = r / NBIN;
+        size_t row;
+        if (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U)
+            row = (size_t)a * N + l;                                             // S[ky=a][kz=l]
+        else if (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN) row = (size_t)l * N + a;  // W[z=l][ky=a]
+        else row = (size_t)a * N + l;                                            // W[z=a][y=l]
+        const cpx<T>* src = (b == 0) ? in0 : in1;
+        cpx<T> v = zero_c<T>();
+        if (q < 3 * ncol) v = src[row * nxp3 + (size_t)kx0 * 3 + q];
+        const int bdst = (MODE == CM_IZ_VEL) ? 1 : b;  // w^ goes to slot 1
+        tile[l * PR + bdst * W + q] = v;
+    }
+    __syncthreads();
+
+    // ---- prologue: u^ = i k x w^ / k^2 for 0 < k^2 <= kM^2 ---------------
+    if constexpr (MODE == CM_IZ_VEL || MODE == CM_IZ_U) {
+        constexpr int WSRC = (MODE == CM_IZ_VEL) ? W : 0;  // slot holding w^
+        const double ky = kwrap<N>(a, kp.dky);
+        for (int e = tid; e < N * TKX; e += COL_THREADS) {
+            const int col = e % TKX;
+            const int l = e / TKX;
+            const double kz = kwrap<N>(l, kp.dkz);
+            const double kx = (double)(kx0 + col) * kp.dkx;
+            const double k2 = (kx * kx + ky * ky) + kz * kz;
+            cpx<T>* w = &tile[l * PR + WSRC + col * 3];
+            cpx<T> u[3];
+            if (k2 <= kp.kM2 && k2 > 0.0) {
+                const T ik2 = (T)(1.0 / k2);
+                cpx<T> wv[3] = {w[0], w[1], w[2]};
+                curl<T>((T)kx, (T)ky, (T)kz, wv, u);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) u[c] = scale(u[c], ik2);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) u[c] = zero_c<T>();
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) tile[l * PR + col * 3 + c] = u[c];
+        }
+        __syncthreads();
+    }
+
+    // ---- FFT along l: NB*W pencils, pencil stride 1, element stride PR ----
+    dif<T, N, INV, NB * W, 1, PR, true, N>(tile, tw, tid, COL_THREADS);
+
+    // ---- epilogue ------------------------------------------------------
+    if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
+        const double ky = kwrap<N>(a, kp.dky);
+        const int nxv = kp.nxv;
+        for (int e = tid; e < N * TKX; e += COL_THREADS) {
+            const int col = e % TKX;
+            const int l = e / TKX;  // output kz index
+            if (col >= ncol) continue;
+            const int ix = kx0 + col;
+            const double kz = kwrap<N>(l, kp.dkz);
+            const double kx = (double)ix * kp.dkx;
+            const double k2 = (kx * kx + ky * ky) + kz * kz;
+            const int p = dif_position<N>(l);
+            cpx<T> nl[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) nl[c] = tile[p * PR + col * 3 + c];
+            // dealias (kspace.cpp:461-485)
+            if (kp.dealias == 1) {
+                int key = (int)rint(k2 * kp.inv_dk2);
+                key = key < kp.nfilt ? key : kp.nfilt - 1;
+                const T f = filt[key];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) nl[c] = scale(nl[c], f);
+            } else if (k2 >= kp.kM2) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) nl[c] = zero_c<T>();
+            }
+            // i k x (vorticity_equation.cpp:323-350)
+            cpx<T> t[3];
+            curl<T>((T)kx, (T)ky, (T)kz, nl, t);
+            const size_t pt = ((size_t)a * N + l) * kp.nxp + ix;  // S[ky=a][kz=l][kx]
+            // forcing (vorticity_equation.cpp:241-288), factor 1
+            if (kp.forcing == 1) {
+                const double kn = sqrt(k2);
+                if (kp.fk0 <= kn && kp.fk1 >= kn) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const cpx<T> fv = fsrc[pt * 3 + c];
+                        t[c].x += (T)(kp.famp * (double)fv.x);
+                        t[c].y += (T)(kp.famp * (double)fv.y);
+                    }
+                }
+            } else if (kp.forcing == 2) {
+                if (ix == 0 && l == 0) {
+                    if (a == kp.fmode) t[2].x -= (T)(kp.famp / 2);
+                    if (a == N - kp.fmode) t[2].x -= (T)(kp.famp / 2);
+                }
+            }
+            // force_divfree on the nonlinear term; zero mode cleared
+            const bool kzero = (a == 0 && l == 0 && ix == 0);
+            if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), t);
+            if (kzero) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) t[c] = zero_c<T>();
+            }
+            // RK update (vorticity_equation.cpp:366-434), only for k2 <= kM2
+            const bool inside = k2 <= kp.kM2;
+            const T dt = (T)kp.dt;
+            cpx<T> o[3];
+            const int nfac = nxv + 2 * N;
+            if (MODE == CM_FZ_RK1) {
+                const T f0 = fac[ix] * fac[nxv + a] * fac[nxv + N + l];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const cpx<T> v0 = rk_v0[pt * 3 + c];
+                    o[c] = inside ? mk<T>((v0.x + dt * t[c].x) * f0, (v0.y + dt * t[c].y) * f0)
+                                  : zero_c<T>();
+                }
+            } else if (MODE == CM_FZ_RK2) {
+                const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
+                const T f1 = fac[2 * nfac + ix] * fac[2 * nfac + nxv + a] *
+                             fac[2 * nfac + nxv + N + l];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const cpx<T> v0 = rk_v0[pt * 3 + c];
+                    const cpx<T> v1 = rk_vp[pt * 3 + c];
+                    o[c] = inside ? mk<T>((3 * v0.x * f0 + (v1.x + dt * t[c].x) * f1) * (T)0.25,
+                                          (3 * v0.y * f0 + (v1.y + dt * t[c].y) * f1) * (T)0.25)
+                                  : zero_c<T>();
+                }
+            } else {
+                const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const cpx<T> v0 = rk_v0[pt * 3 + c];
+                    const cpx<T> v2 = rk_vp[pt * 3 + c];
+                    o[c] = inside ? mk<T>((v0.x * f0 + 2 * (v2.x + dt * t[c].x)) * f0 / (T)3,
+                                          (v0.y * f0 + 2 * (v2.y + dt * t[c].y)) * f0 / (T)3)
+                                  : v0;
+                }
+                // final force_divfree of the state (vorticity_equation.cpp:436)
+                if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), o);
+                if (kzero) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) out0[pt * 3 + c] = o[c];
+        }
+    } else {
+        // plain store of NB buffers, output row index lo (natural order)
+        for (int e = tid; e < N * NB * W; e += COL_THREADS) {
+            const int q = e % W;
+            const int r = e / W;
+            const int b = r % NB;
+            const int lo = r / NB;
+            if (q >= 3 * ncol) continue;
+            size_t row;
+            if (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U)
+                row = (size_t)lo * N + a;                                            // W[z=lo][ky=a]
+            else if (MODE == CM_FZ_PLAIN) row = (size_t)a * N + lo;                  // S[ky=a][kz=lo]
+            else row = (size_t)a * N + lo;                                           // W[z=a][y=lo]
+            const int p = dif_position<N>(lo);
+            cpx<T>* dst = (b == 0) ? out0 : out1;
+            dst[row * nxp3 + (size_t)kx0 * 3 + q] = tile[p * PR + b * W + q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row pass over (z, y) rows of W.  Shared memory: pencils of length
+// PL = N/2 + 1 (+1 pad), buffer-major: pencil (b*3*ROWS + r*3 + c).
+enum RowMode {
+    RM_NONLIN = 0,     // (u^, w^) rows -> R2C(u x w / N^3) into out, opt. real u
+    RM_C2R = 1,        // complex rows -> real rows
+    RM_R2C = 2,        // real rows -> complex rows
+};
+constexpr int ROW_THREADS = 256;
+
+template <typename T, int N>
+__host__ __device__ constexpr int row_rows() {
+    // about 64 KB of pencils, and at least ~2 CTAs per SM of work
+    return (pow2floor(65536 / (6 * (N / 2 + 2) * (int)sizeof(cpx<T>))) <
+            pow2floor(N * N / 296 > 0 ? N * N / 296 : 1))
+               ? pow2floor(65536 / (6 * (N / 2 + 2) * (int)sizeof(cpx<T>)))
+               : pow2floor(N * N / 296 > 0 ? N * N / 296 : 1);
+}
+template <int N>
+__host__ __device__ constexpr int row_pl() { return N / 2 + 2; }
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr size_t row_smem_bytes() {
+    return (size_t)((MODE == RM_NONLIN ? 6 : 3) * row_rows<T, N>() * row_pl<N>() + N) *
+           sizeof(cpx<T>);
+}
+
+// C2R pre-processing of one pencil (k, M-k pairs), X[0], X[M] real parts.
+template <typename T, int N>
+__device__ __forceinline__ void c2r_pre(cpx<T>* s, const cpx<T>* tw, int k) {
+    constexpr int M = N / 2;
+    if (k == 0) {
+        const T x0 = s[0].x, xm = s[M].x;
+        s[0] = mk<T>(x0 + xm, x0 - xm);
+        return;
+    }
+    const cpx<T> a = s[k], b = s[M - k];
+    const cpx<T> w = tw[k];  // exp(-2 pi i k / N)
+    // Z[k] = (a + conj b) + i conj(w) (a - conj b)
+    {
+        const cpx<T> sp = a + conjg(b), dm = a - conjg(b);
+        const cpx<T> e = cmulc(dm, w);  // dm * conj(w)
+        s[k] = mk<T>(sp.x - e.y, sp.y + e.x);
+    }
+    if (k != M - k) {
+        // Z[M-k] = (b + conj a) - i w (b - conj a)
+        const cpx<T> sp = b + conjg(a), dm = b - conjg(a);
+        const cpx<T> e = cmul(dm, w);
+        s[M - k] = mk<T>(sp.x + e.y, sp.y - e.x);
+    }
+}
+
+// R2C post-processing of one pencil (natural-order Z), writes X[0..M].
+template <typename T, int N>
+__device__ __forceinline__ void r2c_post(cpx<T>* s, const cpx<T>* tw, int k) {
+    constexpr int M = N / 2;
+    const T h = (T)0.5;
+    if (k == 0) {
+        const cpx<T> z0 = s[0];
+        s[0] = mk<T>(z0.x + z0.y, (T)0);
+        s[M] = mk<T>(z0.x - z0.y, (T)0);
+        return;
+    }
+    const cpx<T> zk = s[k], zm = s[M - k];
+    const cpx<T> w = tw[k];
+    {
+        const cpx<T> e = scale(zk + conjg(zm), h);
+        const cpx<T> d = zk - conjg(zm);
+        const cpx<T> o = mk<T>(d.y * h, -d.x * h);  // d / (2i)
+        s[k] = e + cmul(w, o);
+    }
+    if (k != M - k) {
+        // exp(-2 pi i (M-k)/N) = -conj(w)
+        const cpx<T> e = scale(zm + conjg(zk), h);
+        const cpx<T> d = zm - conjg(zk);
+        const cpx<T> o = mk<T>(d.y * h, -d.x * h);
+        s[M - k] = e - cmul(conjg(w), o);
+    }
+}
+
+template <typename T, int N, int MODE, bool WRITE_RU>
+__global__ void __launch_bounds__(ROW_THREADS)
+row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restrict__ ww,
+         cpx<T>* wout, T* __restrict__ rout, const T* __restrict__ rin,
+         const cpx<T>* __restrict__ tw_g) {
+    constexpr int M = N / 2;
+    constexpr int ROWS = row_rows<T, N>();
+    constexpr int PL = row_pl<N>();
+    constexpr int NBIN = (MODE == RM_NONLIN) ? 2 : 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* S = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* tw = S + (MODE == RM_NONLIN ? 6 : 3) * ROWS * PL;
+    const int tid = threadIdx.x;
+    const size_t row0 = (size_t)blockIdx.x * ROWS;
+    const int nxv = kp.nxv;
+    const size_t nxp3 = (size_t)kp.nxp * 3;
+
+    for (int i = tid; i < N; i += ROW_THREADS) tw[i] = tw_g[i];
+
+    if constexpr (MODE == RM_R2C) {
+        // real rows into digit-reversed complex pencils z[n] = (x[2n], x[2n+1])
+        for (int e = tid; e < ROWS * 3 * M; e += ROW_THREADS) {
+            const int c = e % 3;
+            const int r2 = e / 3;
+            const int n = r2 % M;
+            const int r = r2 / M;
+            const T* src = rin + ((row0 + r) * N + 2 * n) * 3 + c;
+            S[(r * 3 + c) * PL + dif_position<M>(n)] = mk<T>(src[0], src[3]);
+        }
+        __syncthreads();
+    } else {
+        for (int e = tid; e < ROWS * NBIN * nxv * 3; e += ROW_THREADS) {
+            const int q = e % (nxv * 3);
+            const int r2 = e / (nxv * 3);
+            const int b = r2 % NBIN;
+            const int r = r2 / NBIN;
+            const cpx<T>* src = (b == 0) ? wu : ww;
+            const int kx = q / 3, c = q % 3;
+            S[(b * 3 * ROWS + r * 3 + c) * PL + kx] = src[(row0 + r) * nxp3 + q];
+        }
+        __syncthreads();
+        constexpr int NP = NBIN * 3 * ROWS;
+        for (int e = tid; e < NP * (M / 2 + 1); e += ROW_THREADS) {
+            const int k = e % (M / 2 + 1);
+            const int p = e / (M / 2 + 1);
+            c2r_pre<T, N>(S + p * PL, tw, k);
+        }
+        __syncthreads();
+        dif<T, M, true, NP, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
+
+        if constexpr (MODE == RM_C2R || WRITE_RU) {
+            // real u (first 3*ROWS pencils) to rout, natural x order
+            for (int e = tid; e < ROWS * N * 3; e += ROW_THREADS) {
+                const int c = e % 3;
+                const int r2 = e / 3;
+                const int x = r2 % N;
+                const int r = r2 / N;
+                const cpx<T> z = S[(r * 3 + c) * PL + dif_position<M>(x >> 1)];
+                rout[((row0 + r) * N + x) * 3 + c] = (x & 1) ? z.y : z.x;
+            }
+            if constexpr (MODE == RM_C2R) return;
+            __syncthreads();
+        }
+        if constexpr (MODE == RM_NONLIN) {
+            // u x w / npoints at each position (two grid points per position)
+            const T inv_np = (T)1 / ((T)N * (T)N * (T)N);
+            for (int e = tid; e < ROWS * M; e += ROW_THREADS) {
+                const int p = e % M;
+                const int r = e / M;
+                cpx<T> u[3], w[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    u[c] = S[(r * 3 + c) * PL + p];
+                    w[c] = S[(3 * ROWS + r * 3 + c) * PL + p];
+                }
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc) {
+                    const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+                    const T tx = u[c1].x * w[c2].x - u[c2].x * w[c1].x;
+                    const T ty = u[c1].y * w[c2].y - u[c2].y * w[c1].y;
+                    S[(r * 3 + cc) * PL + p] = mk<T>(tx * inv_np, ty * inv_np);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // forward: digit-reversed -> natural, then R2C post-processing
+    dit<T, M, false, 3 * ROWS, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
+    for (int e = tid; e < 3 * ROWS * (M / 2 + 1); e += ROW_THREADS) {
+        const int k = e % (M / 2 + 1);
+        const int p = e / (M / 2 + 1);
+        r2c_post<T, N>(S + p * PL, tw, k);
+    }
+    __syncthreads();
+    for (int e = tid; e < ROWS * nxv * 3; e += ROW_THREADS) {
+        const int q = e % (nxv * 3);
+        const int r = e / (nxv * 3);
+        const int kx = q / 3, c = q % 3;
+        wout[(row0 + r) * nxp3 + q] = S[(r * 3 + c) * PL + kx];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// field::symmetrize on the kx = 0 plane of a state-layout buffer
+// (field.cpp:903-978).  One thread per (ky, kz) of the plane.
+template <typename T, int N>
+__global__ void symmetrize_kernel(cpx<T>* s, int nxp) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= N * N) return;
+    const int ky = e / N, kz = e % N;
+    const size_t P = (size_t)nxp;
+    auto at = [&](int y, int z) -> cpx<T>* { return s + ((size_t)y * N + z) * P * 3; };
+    if (ky == 0) {
+        if (kz == 0) {
+            cpx<T>* d = at(0, 0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) d[c].y = (T)0;
+        } else if (kz > N / 2) {
+            // a[0][N-ii] = conj(a[0][ii]), ii = N - kz in 1..N/2-1
+            const cpx<T>* src = at(0, N - kz);
+            cpx<T>* d = at(0, kz);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) d[c] = conjg(src[c]);
+        }
+    } else if (ky > N / 2) {
+        const int yy = N - ky;  // 1..N/2-1
+        const int src_kz = (kz == 0) ? 0 : N - kz;
+        const cpx<T>* src = at(yy, src_kz);
+        cpx<T>* d = at(ky, kz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) d[c] = conjg(src[c]);
+    }
+}
+
+// pointwise k-space kernels over the state layout ----------------------------
+// compute_velocity (vorticity_equation.cpp:206-239), without the symmetrize
+template <typename T, int N>
+__global__ void velocity_kernel(const KParams kp, const cpx<T>* __restrict__ w, cpx<T>* u) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t npts = (size_t)N * N * kp.nxv;
+    if (e >= npts) return;
+    const int ix = (int)(e % kp.nxv);
+    const size_t r = e / kp.nxv;
+    const int kz_i = (int)(r % N), ky_i = (int)(r / N);
+    const double kx = ix * kp.dkx, ky = kwrap<N>(ky_i, kp.dky), kz = kwrap<N>(kz_i, kp.dkz);
+    const double k2 = (kx * kx + ky * ky) + kz * kz;
+    const size_t pt = r * kp.nxp + ix;
+    cpx<T> o[3];
+    if (k2 <= kp.kM2 && k2 > 0.0) {
+        cpx<T> wv[3] = {w[pt * 3], w[pt * 3 + 1], w[pt * 3 + 2]};
+        curl<T>((T)kx, (T)ky, (T)kz, wv, o);
+        const T ik2 = (T)(1.0 / k2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[c] = scale(o[c], ik2);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[pt * 3 + c] = o[c];
+}
+
+// low_pass(kM) + force_divfree (vorticity_equation.hpp:121-126)
+template <typename T, int N>
+__global__ void lowpass_divfree_kernel(const KParams kp, cpx<T>* a) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t npts = (size_t)N * N * kp.nxv;
+    if (e >= npts) return;
+    const int ix = (int)(e % kp.nxv);
+    const size_t r = e / kp.nxv;
+    const int kz_i = (int)(r % N), ky_i = (int)(r / N);
+    const double kx = ix * kp.dkx, ky = kwrap<N>(ky_i, kp.dky), kz = kwrap<N>(kz_i, kp.dkz);
+    const double k2 = (kx * kx + ky * ky) + kz * kz;
+    const size_t pt = r * kp.nxp + ix;
+    cpx<T> v[3] = {a[pt * 3], a[pt * 3 + 1], a[pt * 3 + 2]};
+    if (k2 >= kp.kM2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = zero_c<T>();
+    }
+    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), v);
+    if (e == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = zero_c<T>();
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a[pt * 3 + c] = v[c];
+}
+
+}  // namespace bfg

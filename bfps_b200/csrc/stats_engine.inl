@@ -1,0 +1,50 @@
+// Engine<T, N>::stats — field::compute_stats (bfps/cpp/field.cpp:984-1040)
+// for one complex 3-vector field in the state layout: co-spectrum, then the
+// unnormalised C2R into scratch (v2 is free between steps: every step
+// rewrites it completely) and the real-space moments and histograms.
+// Included by bfps_b200.cu after the Engine definition.
+
+template <typename T, int N>
+int Engine<T, N>::stats(bfg_ctx* c, const void* cfield, double max_est, int nbins, double* spec,
+                        double* mom, int64_t* hist) {
+    const size_t spec_n = (size_t)c->nshells * 9;
+    const size_t need = spec_n * 8 + (size_t)STATS_BLOCKS * NQ * 8 + NQ * 8 +
+                        (size_t)nbins * 4 * 8;
+    if (c->stats_ws_bytes < need) {
+        if (c->stats_ws) cudaFree(c->stats_ws);
+        c->stats_ws = nullptr;
+        c->stats_ws_bytes = 0;
+        CU(cudaMalloc(&c->stats_ws, need));
+        c->stats_ws_bytes = need;
+    }
+    double* d_spec = (double*)c->stats_ws;
+    double* d_part = d_spec + spec_n;
+    double* d_mom = d_part + (size_t)STATS_BLOCKS * NQ;
+    unsigned long long* d_hist = (unsigned long long*)(d_mom + NQ);
+    CU(cudaMemsetAsync(d_spec, 0, spec_n * 8, c->stream));
+    CU(cudaMemsetAsync(d_hist, 0, (size_t)nbins * 4 * 8, c->stream));
+    const KParams kp = kparams(c, 0.0);
+    Prof pr0(c, K_STATS);
+    spectrum_kernel<T, N><<<STATS_BLOCKS, 256, spec_n * 8, c->stream>>>(
+        kp, (const C*)cfield, c->nshells, c->dk, d_spec);
+    int rc = after_launch(c, "spectrum");
+    if (rc) return rc;
+    // real-space field into v2 (as [z][y][x][3] reals)
+    if ((rc = col<CM_IZ_PLAIN>(c, 0.0, cfield, nullptr, c->wb, nullptr))) return rc;
+    if ((rc = col<CM_Y_INV1>(c, 0.0, c->wb, nullptr, c->wb, nullptr))) return rc;
+    if ((rc = row<RM_C2R, false>(c, c->wb, nullptr, nullptr, c->v2, nullptr))) return rc;
+    const double me3 = max_est * std::sqrt(3.0);
+    const size_t npts = (size_t)N * N * N;
+    CU(ensure_smem(moments_kernel<T>, (size_t)nbins * 4 * 4, c->device));
+    Prof pr1(c, K_STATS);
+    moments_kernel<T><<<STATS_BLOCKS, STATS_THREADS, (size_t)nbins * 4 * 4, c->stream>>>(
+        (const T*)c->v2, npts, max_est, max_est, max_est, me3, nbins, d_part, d_hist);
+    if ((rc = after_launch(c, "moments"))) return rc;
+    moments_final<<<1, 64, 0, c->stream>>>(d_part, STATS_BLOCKS, 1.0 / (double)npts, d_mom);
+    if ((rc = after_launch(c, "moments_final"))) return rc;
+    if (spec) CU(cudaMemcpyAsync(spec, d_spec, spec_n * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (mom) CU(cudaMemcpyAsync(mom, d_mom, NQ * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (hist) CU(cudaMemcpyAsync(hist, d_hist, (size_t)nbins * 4 * 8, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}

@@ -1,0 +1,245 @@
+"""Host-side mirror of bfps' building blocks over the C-ABI.
+
+``vorticity_equation`` mirrors ``vorticity_equation<rnumber, FFTW>``
+(bfps/cpp/vorticity_equation.hpp:46-134): public physical members, step(),
+compute_velocity(), the io_checkpoint read semantics, and the iteration
+counter.  ``particles_system`` mirrors ``abstract_particles_system``
+(bfps/cpp/particles/abstract_particles_system.hpp:12-55) with
+completeLoop(), and ``NSVEparticles_step`` is NSVEparticles::step
+(bfps/cpp/full_code/NSVEparticles.cpp:33-41).  Fields cross the boundary in
+the reference's host layouts (bfps/cpp/field.cpp:85-101).
+
+All compute runs in the CUDA library; every method raises on failure.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr
+
+
+class vorticity_equation:
+    def __init__(self, nx, ny=None, nz=None, dkx=1.0, dky=1.0, dkz=1.0,
+                 precision="double", dealias_type=_lib.SMOOTH, device=0):
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.real_bytes = {"single": 4, "double": 8}[precision]
+        self.rdtype = np.float32 if self.real_bytes == 4 else np.float64
+        self.cdtype = np.complex64 if self.real_bytes == 4 else np.complex128
+        h = ctypes.c_void_p()
+        rc = lib().bfg_ctx_create(ctypes.byref(h), nx, ny, nz, dkx, dky, dkz,
+                                  self.real_bytes, dealias_type, device)
+        if rc != 0:
+            raise _lib.BfgError(rc, "bfg_ctx_create(%d, %d, %d, precision=%s)" %
+                                (nx, ny, nz, precision))
+        self._h = h
+        # defaults of the reference constructor (vorticity_equation.cpp:150-155)
+        self._nu = 0.1
+        self._forcing_type = "none"
+        self._famplitude = 1.0
+        self._fk0 = 2.0
+        self._fk1 = 4.0
+        self._fmode = 1
+        self._push_physics()
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bfg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- physical members ---------------------------------------------------
+    def _push_physics(self):
+        check(lib().bfg_set_physics(self._h, self._nu, _lib.FORCING[self._forcing_type],
+                                    self._famplitude, self._fk0, self._fk1, self._fmode), self._h)
+
+    def _prop(name):
+        def get(self):
+            return getattr(self, "_" + name)
+
+        def set_(self, v):
+            setattr(self, "_" + name, v)
+            self._push_physics()
+        return property(get, set_)
+
+    nu = _prop("nu")
+    forcing_type = _prop("forcing_type")
+    famplitude = _prop("famplitude")
+    fk0 = _prop("fk0")
+    fk1 = _prop("fk1")
+    fmode = _prop("fmode")
+    del _prop
+
+    @property
+    def iteration(self):
+        it = ctypes.c_int()
+        check(lib().bfg_get_iteration(self._h, ctypes.byref(it)), self._h)
+        return it.value
+
+    @iteration.setter
+    def iteration(self, v):
+        check(lib().bfg_set_iteration(self._h, int(v)), self._h)
+
+    # -- kspace --------------------------------------------------------------
+    def kspace(self):
+        kM, dk, ns = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        check(lib().bfg_kspace_info(self._h, ctypes.byref(kM), ctypes.byref(dk),
+                                    ctypes.byref(ns), None, None), self._h)
+        kshell = np.zeros(ns.value)
+        nshell = np.zeros(ns.value, np.int64)
+        check(lib().bfg_kspace_info(self._h, None, None, None, ptr(kshell),
+                                    ptr(nshell, ctypes.c_int64)), self._h)
+        return dict(kM=kM.value, dk=dk.value, nshells=ns.value, kshell=kshell, nshell=nshell)
+
+    # -- fields ----------------------------------------------------------------
+    @property
+    def cshape(self):
+        return (self.ny, self.nz, self.nx // 2 + 1, 3)
+
+    @property
+    def rshape(self):
+        return (self.nz, self.ny, self.nx + 2, 3)
+
+    def set_cvorticity(self, a):
+        a = np.ascontiguousarray(a, dtype=self.cdtype)
+        assert a.shape == self.cshape, a.shape
+        check(lib().bfg_field_upload(self._h, _lib.FIELD_VORTICITY, a.ctypes.data), self._h)
+
+    def get_cvorticity(self):
+        out = np.empty(self.cshape, self.cdtype)
+        check(lib().bfg_field_download(self._h, _lib.FIELD_VORTICITY, out.ctypes.data), self._h)
+        return out
+
+    def get_cvelocity(self):
+        out = np.empty(self.cshape, self.cdtype)
+        check(lib().bfg_field_download(self._h, _lib.FIELD_VELOCITY, out.ctypes.data), self._h)
+        return out
+
+    def get_rvelocity(self):
+        out = np.empty(self.rshape, self.rdtype)
+        check(lib().bfg_field_download(self._h, _lib.FIELD_RVELOCITY, out.ctypes.data), self._h)
+        return out
+
+    def set_rvelocity(self, r):
+        r = np.ascontiguousarray(r, dtype=self.rdtype)
+        assert r.shape == self.rshape
+        check(lib().bfg_field_upload(self._h, _lib.FIELD_RVELOCITY, r.ctypes.data), self._h)
+
+    def io_checkpoint_read(self, a):
+        """Upload a checkpoint field and apply io_checkpoint(read) semantics
+        (vorticity_equation.hpp:107-128): symmetrize, low_pass(kM), force_divfree."""
+        self.set_cvorticity(a)
+        check(lib().bfg_read_checkpoint_fixup(self._h), self._h)
+
+    # -- solver ------------------------------------------------------------------
+    def step(self, dt, nsteps=1):
+        check(lib().bfg_step(self._h, float(dt), int(nsteps)), self._h)
+
+    def compute_velocity(self):
+        check(lib().bfg_compute_velocity(self._h), self._h)
+
+    def velocity_rspace(self):
+        check(lib().bfg_velocity_rspace(self._h), self._h)
+
+    def last_step_ms(self):
+        ms = ctypes.c_double()
+        check(lib().bfg_last_step_ms(self._h, ctypes.byref(ms)), self._h)
+        return ms.value
+
+    def kernel_launches(self):
+        n = ctypes.c_int64()
+        check(lib().bfg_kernel_launches(self._h, ctypes.byref(n)), self._h)
+        return n.value
+
+    def do_stats(self, max_velocity_estimate=1.0, max_vorticity_estimate=1.0, nbins=256):
+        """NSVE::do_stats (NSVE.cpp:101-135) results as numpy arrays."""
+        ns = self.kspace()["nshells"]
+        sv, sw = np.zeros((ns, 3, 3)), np.zeros((ns, 3, 3))
+        mv, mw = np.zeros((10, 4)), np.zeros((10, 4))
+        hv, hw = np.zeros((nbins, 4), np.int64), np.zeros((nbins, 4), np.int64)
+        check(lib().bfg_stats(self._h, max_velocity_estimate, max_vorticity_estimate, nbins,
+                              ptr(sv), ptr(sw), ptr(mv), ptr(mw), ptr(hv, ctypes.c_int64),
+                              ptr(hw, ctypes.c_int64)), self._h)
+        return {"velocity": (sv, mv, hv), "vorticity": (sw, mw, hw)}
+
+
+class particles_system:
+    """Tracers on the device (particles_system_builder + particles_system)."""
+
+    def __init__(self, fs, pos, neighbours, smoothness, nsteps, rhs=None, idx=None, step_idx=1):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        n = pos.shape[0]
+        if rhs is not None:
+            rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+            assert rhs.shape == (nsteps, n, 3)
+        if idx is not None:
+            idx = np.ascontiguousarray(idx, dtype=np.int64)
+        h = ctypes.c_void_p()
+        check(lib().bfg_particles_create(fs.handle, ctypes.byref(h), n, neighbours, smoothness,
+                                         nsteps, ptr(pos), ptr(rhs), ptr(idx, ctypes.c_int64),
+                                         step_idx), fs.handle)
+        self._h = h
+        self.fs = fs
+        self.n = n
+        self.nsteps = nsteps
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bfg_particles_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def completeLoop(self, dt):
+        check(lib().bfg_particles_complete_loop(self._h, float(dt)), self.fs.handle)
+
+    def sample_velocity(self):
+        out = np.empty((self.n, 3))
+        check(lib().bfg_particles_sample_velocity(self._h, ptr(out)), self.fs.handle)
+        return out
+
+    def state(self):
+        pos = np.empty((self.n, 3))
+        rhs = np.empty((self.nsteps, self.n, 3))
+        idx = np.empty(self.n, np.int64)
+        check(lib().bfg_particles_download(self._h, ptr(pos), ptr(rhs),
+                                           ptr(idx, ctypes.c_int64)), self.fs.handle)
+        return pos, rhs, idx
+
+    @property
+    def step_idx(self):
+        s = ctypes.c_int()
+        check(lib().bfg_particles_info(self._h, None, None, ctypes.byref(s)), self.fs.handle)
+        return s.value
+
+
+def NSVEparticles_step(fs, ps, dt, nsteps=1):
+    """NSVEparticles::step (NSVEparticles.cpp:33-41), nsteps times."""
+    check(lib().bfg_nsveparticles_step(fs.handle, ps.handle if ps is not None else None,
+                                       float(dt), int(nsteps)), fs.handle)

@@ -1,0 +1,188 @@
+/*
+ * bfps_b200 — single-GPU (B200, sm_100a) engine for bfps' pseudospectral
+ * vorticity-equation DNS step and Lagrangian tracer step.
+ *
+ * C ABI: plain pointers and sizes only; no exceptions cross it.  Every entry
+ * point returns 0 on success or a negative BFG_E* code; the message of the
+ * most recent failure on a context is kept until the next call
+ * (bfg_last_error).  One host thread drives a context (the reference is
+ * MPI_THREAD_FUNNELED with OpenMP inside calls, main_code.hpp:74-96);
+ * distinct contexts may be driven from distinct threads.
+ *
+ * Memory layouts at the boundary are exactly the reference's host layouts
+ * (bfps/cpp/field.cpp:85-101):
+ *   complex 3-vector field: [ky][kz][kx][c][re,im], kx in 0..nx/2
+ *                           ("transposed out", shape (ny, nz, nx/2+1, 3))
+ *   real 3-vector field:    [z][y][x][c] with x padded to nx+2
+ *                           (shape (nz, ny, nx+2, 3); the pad is written as 0)
+ *   tracers:                positions (n, 3) f64, rhs history (nsteps, n, 3)
+ *                           f64, indices (n) i64, in global index order
+ *                           (particles_output_hdf5.hpp).
+ * Scalars are float when real_bytes == 4 and double when real_bytes == 8.
+ */
+#ifndef BFPS_B200_H
+#define BFPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bfg_ctx bfg_ctx;
+typedef struct bfg_pctx bfg_pctx;
+
+/* error codes */
+#define BFG_OK 0
+#define BFG_EINVAL -1     /* bad argument */
+#define BFG_ECUDA -2      /* CUDA runtime error */
+#define BFG_ENOMEM -3     /* device allocation failed */
+#define BFG_EUNSUP -4     /* configuration not supported by this build */
+#define BFG_ESTATE -5     /* call not valid in the current state */
+
+/* dealiasing (bfps/cpp/kspace.hpp:40, enum kspace_dealias_type) */
+#define BFG_TWO_THIRDS 0
+#define BFG_SMOOTH 1
+
+/* forcing_type (bfps/cpp/vorticity_equation.cpp:241-288) */
+#define BFG_FORCING_NONE 0
+#define BFG_FORCING_LINEAR 1
+#define BFG_FORCING_KOLMOGOROV 2
+
+/* field ids for upload / download */
+#define BFG_FIELD_VORTICITY 0   /* complex state, vorticity_equation::cvorticity */
+#define BFG_FIELD_VELOCITY 1    /* complex, vorticity_equation::cvelocity */
+#define BFG_FIELD_RVELOCITY 2   /* real velocity, cvelocity after ift() */
+
+/* Library version string. */
+const char* bfg_version(void);
+
+/* Create a solver context: replaces the constructors of
+ * vorticity_equation<rnumber, FFTW> (bfps/cpp/vorticity_equation.cpp:110-156)
+ * with its five field<rnumber, FFTW, THREE> buffers (field.cpp:37-121) and
+ * kspace<FFTW, dt> (kspace.cpp:34-167).  Grids are cubic, nx = ny = nz = n,
+ * n a power of two in [16, 1024].  real_bytes selects rnumber (4 or 8).
+ * The state starts at zero with iteration 0 and the reference constructor's
+ * physical defaults (nu 0.1, forcing none). */
+int bfg_ctx_create(bfg_ctx** out, int nx, int ny, int nz, double dkx, double dky,
+                   double dkz, int real_bytes, int dealias_type, int device);
+void bfg_ctx_destroy(bfg_ctx* ctx);
+const char* bfg_last_error(const bfg_ctx* ctx);
+
+/* Physical parameters: the public members nu, forcing_type, famplitude,
+ * fk0, fk1, fmode of vorticity_equation (vorticity_equation.hpp:46-134). */
+int bfg_set_physics(bfg_ctx* ctx, double nu, int forcing_type, double famplitude,
+                    double fk0, double fk1, int fmode);
+
+/* kspace information (kspace.hpp:43-60): kM, dk, nshells; kshell / nshell
+ * arrays of length nshells may be NULL. */
+int bfg_kspace_info(const bfg_ctx* ctx, double* kM, double* dk, int* nshells,
+                    double* kshell, int64_t* nshell);
+
+/* Host <-> device copies in the reference layouts above.
+ * Upload of BFG_FIELD_VORTICITY replaces the state; it does NOT apply the
+ * checkpoint-read transformations (use bfg_read_checkpoint_fixup). */
+int bfg_field_upload(bfg_ctx* ctx, int field_id, const void* host);
+int bfg_field_download(bfg_ctx* ctx, int field_id, void* host);
+
+/* io_checkpoint(read) post-processing of the state
+ * (vorticity_equation.hpp:107-128 with field::io's symmetrize at
+ * field.cpp:340): symmetrize, low_pass(kM), force_divfree. */
+int bfg_read_checkpoint_fixup(bfg_ctx* ctx);
+
+/* vorticity_equation::step (vorticity_equation.cpp:358-439), nsteps times:
+ * one IF-RK3 step each, iteration += 1 each. */
+int bfg_step(bfg_ctx* ctx, double dt, int nsteps);
+
+/* vorticity_equation::compute_velocity(cvorticity)
+ * (vorticity_equation.cpp:206-239): fills BFG_FIELD_VELOCITY. */
+int bfg_compute_velocity(bfg_ctx* ctx);
+
+/* compute_velocity(cvorticity) followed by cvelocity->ift()
+ * (NSVEparticles.cpp:35-36): fills BFG_FIELD_RVELOCITY. */
+int bfg_velocity_rspace(bfg_ctx* ctx);
+
+/* field::ift / field::dft (field.cpp:144-162) on a 3-vector field, using
+ * caller device buffers in the reference layouts (complex: (n, n, n/2+1, 3),
+ * real: (n, n, n+2, 3)); unnormalised like FFTW.  in may equal out. */
+int bfg_ift(bfg_ctx* ctx, const void* dev_complex_in, void* dev_real_out);
+int bfg_dft(bfg_ctx* ctx, const void* dev_real_in, void* dev_complex_out);
+
+/* iteration counter (vorticity_equation::iteration). */
+int bfg_get_iteration(const bfg_ctx* ctx, int* iteration);
+int bfg_set_iteration(bfg_ctx* ctx, int iteration);
+
+/* Field statistics of NSVE::do_stats (bfps/cpp/full_code/NSVE.cpp:101-135)
+ * for the current state: co-spectra (kspace::cospectrum, kspace.cpp:521-598)
+ * of vorticity and velocity, (nshells, 3, 3) f64 each, and real-space
+ * moments (10, 4) f64 and histograms (nbins, 4) i64
+ * (field::compute_rspace_stats, field.cpp:661-889).  max_*_estimate are the
+ * parameters of the same names; any output pointer may be NULL. */
+int bfg_stats(bfg_ctx* ctx, double max_velocity_estimate, double max_vorticity_estimate,
+              int nbins, double* spec_vel, double* spec_vort, double* mom_vel,
+              double* mom_vort, int64_t* hist_vel, int64_t* hist_vort);
+
+/* ---------------------------------------------------------- tracers ---- */
+
+/* particles_system_builder (bfps/cpp/particles/particles_system_builder.hpp:
+ * 111-257) + particles_system::init (particles_system.hpp:81-121):
+ * n tracers, interpolation (neighbours 1..5, smoothness 0..2; 0 = Lagrange),
+ * nsteps >= 1 Adams-Bashforth history slots, step_idx = iteration + 1 of the
+ * run that resumes (NSVEparticles.cpp:23).  pos is (n, 3), rhs is
+ * (nsteps, n, 3) (may be NULL for zeros), idx is (n) (NULL for 0..n-1). */
+int bfg_particles_create(bfg_ctx* ctx, bfg_pctx** out, int64_t n, int neighbours,
+                         int smoothness, int nsteps, const double* pos,
+                         const double* rhs, const int64_t* idx, int step_idx);
+void bfg_particles_destroy(bfg_pctx* p);
+
+/* particles_system::completeLoop(dt) (particles_system.hpp:210-217) using
+ * the context's real velocity field (BFG_FIELD_RVELOCITY). */
+int bfg_particles_complete_loop(bfg_pctx* p, double dt);
+
+/* NSVEparticles::step (bfps/cpp/full_code/NSVEparticles.cpp:33-41):
+ * velocity at time t -> tracers advance -> fluid IF-RK3 step, nsteps times.
+ * p may be NULL (then this is NSVE::step). */
+int bfg_nsveparticles_step(bfg_ctx* ctx, bfg_pctx* p, double dt, int nsteps);
+
+/* Sample the context's real velocity field at the tracer positions
+ * (particles_system::sample_compute, particles_system.hpp:134-170) into
+ * out (n, 3) in global index order. */
+int bfg_particles_sample_velocity(bfg_pctx* p, double* out);
+
+/* Replace positions (n, 3) and the rhs history (nsteps, n, 3, NULL for
+ * zeros) of existing tracers, in the order given at creation, and set
+ * step_idx (checkpoint read, particles_input_hdf5.hpp:61-279). */
+int bfg_particles_upload(bfg_pctx* p, const double* pos, const double* rhs, int step_idx);
+
+/* State in global index order: pos (n, 3), rhs (nsteps, n, 3), idx (n);
+ * any pointer may be NULL. */
+int bfg_particles_download(bfg_pctx* p, double* pos, double* rhs, int64_t* idx);
+int bfg_particles_info(const bfg_pctx* p, int64_t* n, int* nsteps, int* step_idx);
+
+/* ------------------------------------------------------ measurement ---- */
+
+/* Synchronise the context's stream and return the device time of the last
+ * bfg_step / bfg_nsveparticles_step call in milliseconds (CUDA events). */
+int bfg_last_step_ms(bfg_ctx* ctx, double* ms);
+
+/* Per-kernel device timing.  With profiling on, every launch on the
+ * context's stream is bracketed by CUDA events and its duration is added to
+ * its kind: 0 IZ (inverse over kz, fused compute_velocity), 1 IY (inverse
+ * over ky), 2 X (row pass: C2R, u x w, R2C), 3 FY (forward over y),
+ * 4 FZ (forward over z, fused dealias / curl / forcing / divfree / RK),
+ * 5 small k-space kernels, 6 tracers, 7 statistics.  bfg_profile_read
+ * synchronises, returns the accumulated milliseconds and launch count of a
+ * kind, and bfg_profile(ctx, 1) also clears the accumulators. */
+#define BFG_NKINDS 8
+int bfg_profile(bfg_ctx* ctx, int enable);
+int bfg_profile_read(bfg_ctx* ctx, int kind, double* total_ms, int64_t* launches);
+
+/* Count of kernels the library launched since the context was created. */
+int bfg_kernel_launches(const bfg_ctx* ctx, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BFPS_B200_H */

@@ -1,0 +1,64 @@
+"""Tracer gather + Adams-Bashforth on the GPU against the oracle."""
+import numpy as np
+import pytest
+
+from oracle import nsve as O
+from oracle import particles as P
+from oracle.nsveparticles import nsveparticles_step
+from bfps_b200 import ic
+from gpu_util import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nm", [(1, 0), (1, 1), (2, 0), (2, 2), (3, 2), (4, 1), (5, 2)])
+def test_sample_matches_oracle(nm):
+    from bfps_b200.solver import vorticity_equation, particles_system
+    n = 32
+    nb, mm = nm
+    ve = vorticity_equation(n, precision="double")
+    w0 = ic.vorticity_ic(n, seed=1)
+    ve.set_cvorticity(w0)
+    ve.velocity_rspace()
+    ref = O.VorticityEquation(n)
+    ur = ref.ift(ref.compute_velocity(w0))
+    pos = ic.tracer_ic(777, seed=4)
+    pos[:5] = [[0, 0, 0], [2 * np.pi - 1e-12, 0.1, 6.2], [-0.3, 7.0, 13.1], [3.0, 3.0, 3.0], [1e-9, 2.0, -1e-9]]
+    ps = particles_system(ve, pos, nb, mm, nsteps=2)
+    got = ps.sample_velocity()
+    want = P.sample(ur, pos, nb, mm, P.Geometry(n, n, n))
+    assert rel_err(got, want) < 1e-12
+    ps.close()
+    ve.close()
+
+
+@pytest.mark.parametrize("nm,nsteps", [((2, 0), 2), ((2, 2), 4), ((3, 2), 3), ((1, 1), 6)])
+def test_nsveparticles_steps_match_oracle(nm, nsteps):
+    from bfps_b200.solver import vorticity_equation, particles_system, NSVEparticles_step
+    n = 32
+    ve = vorticity_equation(n, precision="double")
+    ref = O.VorticityEquation(n)
+    for obj in (ve, ref):
+        obj.nu = 0.1
+        obj.forcing_type = "linear"
+        obj.famplitude = 0.5
+        obj.fk0 = 1.5
+        obj.fk1 = 3.0
+    w0 = ic.vorticity_ic(n, seed=0)
+    ve.set_cvorticity(w0)
+    ref.cvorticity = w0.copy()
+    pos = ic.tracer_ic(1024, seed=0)
+    ps = particles_system(ve, pos, nm[0], nm[1], nsteps)
+    rps = P.ParticlesSystem(pos, np.zeros((nsteps, 1024, 3)), nm[0], nm[1], P.Geometry(n, n, n))
+    for s in range(8):
+        NSVEparticles_step(ve, ps, 0.01)
+        nsveparticles_step(ref, rps, 0.01)
+    p, r, idx = ps.state()
+    assert np.array_equal(idx, np.arange(1024))
+    assert rel_err(p, rps.pos) < 1e-10
+    assert rel_err(r, rps.rhs) < 1e-10
+    assert np.all(r[0] == 0)
+    assert ps.step_idx == 9
+    assert rel_err(ve.get_cvorticity(), ref.cvorticity) < 1e-10
+    ps.close()
+    ve.close()
