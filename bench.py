@@ -372,8 +372,7 @@ def cpu_baseline(cfg, budget):
     return {"value": round(1.0 / step_s, 6), "unit": "steps/s", "cores": cores, "kind": "port",
             "sample": ("CPU restatement (numpy + scipy.fft, %d workers): one IF-RK3 stage at "
                        "%d^3 timed (%.2f s, x3) + tracer step for %d of %d tracers (%.2f s "
-                       "scaled)" % (cores, cfg["n"], cfg["n"], stage_s, nt, cfg["ntracers"],
-                                    tracer_s))}
+                       "scaled)" % (cores, cfg["n"], stage_s, nt, cfg["ntracers"], tracer_s))}
 
 
 def run_reference(args, cfg):

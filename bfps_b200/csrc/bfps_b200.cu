@@ -25,6 +25,8 @@ using namespace bfg;
 
 struct bfg_ctx {
     int n = 0, nxv = 0, nxp = 0;
+    int nsm = 148;           // streaming multiprocessors (persistent grids)
+    int smem_optin = 0;      // max dynamic shared memory per block
     int real_bytes = 8;
     int dealias = BFG_SMOOTH;
     int device = 0;
@@ -74,10 +76,25 @@ struct bfg_pctx {
     int step_idx = 1;
     int head = 0;
     bool rhs0_zero = true;
+    // device state, in cell order; corder = position of each tracer in the
+    // order given at creation
     double* pos = nullptr;
     double* hist = nullptr;
+    int64_t* corder = nullptr;
+    // second copies for the re-sort, and scratch
+    double* pos2 = nullptr;
+    double* hist2 = nullptr;
+    int64_t* corder2 = nullptr;
     double* sample = nullptr;
-    std::vector<int64_t> idx;  // host copy of the global indices (device order)
+    unsigned* key = nullptr;
+    unsigned* rank = nullptr;
+    unsigned* count = nullptr;
+    unsigned* offset = nullptr;
+    int resort_every = 4;
+    int loops_since_sort = 0;
+    std::vector<int64_t> idx;       // global index of each tracer, creation order
+    std::vector<int64_t> by_index;  // creation positions sorted by global index
+    bool identity = true;           // idx == 0..n-1
 };
 
 // ------------------------------------------------------------ helpers --
@@ -196,8 +213,12 @@ struct Engine {
         constexpr int TKX = col_tkx<T, N, NB>();
         constexpr size_t smem = col_smem_bytes<T, N, MODE>();
         auto kern = col_pass<T, N, MODE>;
+        if (smem > (size_t)c->smem_optin)
+            return fail(c, BFG_EUNSUP, "column pass needs %zu bytes of shared memory", smem);
         CU(ensure_smem(kern, smem, c->device));
-        dim3 grid((c->nxv + TKX - 1) / TKX, N);
+        const int ntx = (c->nxv + TKX - 1) / TKX;
+        const int ntiles = ntx * N;
+        const int grid = std::min(ntiles, c->nsm);
         constexpr int kind = (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) ? K_IZ
                              : (MODE == CM_Y_INV1 || MODE == CM_Y_INV2)                  ? K_IY
                              : (MODE == CM_Y_FWD1)                                      ? K_FY
@@ -206,7 +227,7 @@ struct Engine {
         kern<<<grid, COL_THREADS, smem, c->stream>>>(
             kparams(c, dt), (const C*)in0, (const C*)in1, (C*)out0, (C*)out1, (const C*)v0,
             (const C*)vp, (const C*)fsrc, (const T*)c->filt, (const T*)c->fac,
-            (const C*)c->tw);
+            (const C*)c->tw, ntx, ntiles);
         return after_launch(c, "col_pass");
     }
 
@@ -214,13 +235,17 @@ struct Engine {
     static int row(bfg_ctx* c, const void* wu, const void* ww, void* wout, void* rout,
                    const void* rin) {
         constexpr size_t smem = row_smem_bytes<T, N, MODE>();
-        constexpr int ROWS = row_rows<T, N>();
+        constexpr int ROWS = row_rows<T, N, MODE>();
         auto kern = row_pass<T, N, MODE, WRU>;
+        if (smem > (size_t)c->smem_optin)
+            return fail(c, BFG_EUNSUP, "row pass needs %zu bytes of shared memory", smem);
         CU(ensure_smem(kern, smem, c->device));
+        const int ntiles = N * N / ROWS;
+        const int grid = std::min(ntiles, c->nsm);
         Prof pr(c, K_X);
-        row_pass<T, N, MODE, WRU><<<N * N / ROWS, ROW_THREADS, smem, c->stream>>>(
+        row_pass<T, N, MODE, WRU><<<grid, ROW_THREADS, smem, c->stream>>>(
             kparams(c, 0.0), (const C*)wu, (const C*)ww, (C*)wout, (T*)rout, (const T*)rin,
-            (const C*)c->tw);
+            (const C*)c->tw, ntiles);
         return after_launch(c, "row_pass");
     }
 
@@ -516,8 +541,37 @@ static PParams pparams(const bfg_pctx* p, double dt, int move) {
     return pp;
 }
 
+// counting sort of the tracers by (z, y) cell row (tracer_keys / bucket_scan /
+// tracer_scatter); swaps the state arrays with their second copies
+static int tracer_sort(bfg_pctx* p) {
+    bfg_ctx* c = p->ctx;
+    if (p->n == 0) return 0;
+    const unsigned blocks = (unsigned)((p->n + 255) / 256);
+    const int nb = c->n * c->n;
+    PParams pp = pparams(p, 0.0, 0);
+    Prof pr(c, K_TRACER);
+    CU(cudaMemsetAsync(p->count, 0, (size_t)nb * sizeof(unsigned), c->stream));
+    tracer_keys<<<blocks, 256, 0, c->stream>>>(pp, p->pos, p->key, p->rank, p->count);
+    int rc = after_launch(c, "tracer_keys");
+    if (rc) return rc;
+    bucket_scan<<<1, 1024, 0, c->stream>>>(p->count, p->offset, nb);
+    if ((rc = after_launch(c, "bucket_scan"))) return rc;
+    tracer_scatter<<<blocks, 256, 0, c->stream>>>(pp, p->key, p->rank, p->offset, p->pos, p->hist,
+                                                   p->corder, p->pos2, p->hist2, p->corder2);
+    if ((rc = after_launch(c, "tracer_scatter"))) return rc;
+    std::swap(p->pos, p->pos2);
+    std::swap(p->hist, p->hist2);
+    std::swap(p->corder, p->corder2);
+    p->loops_since_sort = 0;
+    return 0;
+}
+
 static int tracer_loop(bfg_pctx* p, double dt) {
     bfg_ctx* c = p->ctx;
+    if (p->loops_since_sort >= p->resort_every) {
+        int rc = tracer_sort(p);
+        if (rc) return rc;
+    }
     if (p->step_idx > 6 && p->nsteps > 6)
         return fail(c, BFG_EINVAL, "Adams-Bashforth order above 6");
     PParams pp = pparams(p, dt, 1);
@@ -528,6 +582,7 @@ static int tracer_loop(bfg_pctx* p, double dt) {
     p->step_idx += 1;
     p->head = (p->head - 1 + p->nsteps) % p->nsteps;
     p->rhs0_zero = true;
+    p->loops_since_sort += 1;
     return 0;
 }
 
@@ -610,6 +665,10 @@ int bfg_ctx_create(bfg_ctx** out, int nx, int ny, int nz, double dkx, double dky
         return code;
     };
     if (cudaSetDevice(device) != cudaSuccess) return bail(BFG_ECUDA);
+    if (cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) !=
+            cudaSuccess)
+        return bail(BFG_ECUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(BFG_ECUDA);
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
@@ -850,6 +909,42 @@ int bfg_stats(bfg_ctx* c, double max_velocity_estimate, double max_vorticity_est
 }
 
 // ------------------------------------------------------------ tracers --
+// scatter device-order arrays (width doubles per tracer) into creation order
+__global__ void to_creation_order(const double* __restrict__ src, const int64_t* __restrict__ corder,
+                                  int64_t n, int width, double* __restrict__ dst) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t d = corder[i];
+    for (int w = 0; w < width; ++w) dst[d * width + w] = src[i * width + w];
+}
+__global__ void iota64(int64_t* a, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+// device (n, width) array in cell order -> host, global index order
+static int fetch_index_order(bfg_pctx* p, const double* dev, int width, double* out) {
+    bfg_ctx* c = p->ctx;
+    const size_t nw = (size_t)p->n * width;
+    if (p->n == 0) return 0;
+    const unsigned blocks = (unsigned)((p->n + 255) / 256);
+    // pos2 holds n*3 doubles: enough for width <= 3
+    to_creation_order<<<blocks, 256, 0, c->stream>>>(dev, p->corder, p->n, width, p->pos2);
+    int rc = after_launch(c, "to_creation_order");
+    if (rc) return rc;
+    if (p->identity) {
+        CU(cudaMemcpyAsync(out, p->pos2, nw * 8, cudaMemcpyDeviceToHost, c->stream));
+        CU(cudaStreamSynchronize(c->stream));
+        return 0;
+    }
+    std::vector<double> h(nw);
+    CU(cudaMemcpyAsync(h.data(), p->pos2, nw * 8, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    for (int64_t k = 0; k < p->n; ++k)
+        for (int w = 0; w < width; ++w) out[k * width + w] = h[p->by_index[k] * width + w];
+    return 0;
+}
+
 int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, int smoothness,
                          int nsteps, const double* pos, const double* rhs, const int64_t* idx,
                          int step_idx) {
@@ -861,6 +956,7 @@ int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, 
         return fail(c, BFG_EINVAL, "nsteps %d outside 1..6 (particles_adams_bashforth.hpp:24-28)",
                     nsteps);
     if (step_idx < 1) return fail(c, BFG_EINVAL, "step_idx must be >= 1");
+    if (n >= (int64_t)1 << 31) return fail(c, BFG_EUNSUP, "more than 2^31 tracers");
     CU(cudaSetDevice(c->device));
     int rc = ensure_ru(c);
     if (rc) return rc;
@@ -872,44 +968,51 @@ int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, 
     p->nsteps = nsteps;
     p->step_idx = step_idx;
     p->head = 0;
-    const size_t nb = (size_t)std::max<int64_t>(n, 1) * 3 * sizeof(double);
-    if (cudaMalloc(&p->pos, nb) != cudaSuccess || cudaMalloc(&p->hist, nb * nsteps) != cudaSuccess ||
-        cudaMalloc(&p->sample, nb) != cudaSuccess) {
+    const size_t n1 = (size_t)std::max<int64_t>(n, 1);
+    const size_t nb = n1 * 3 * sizeof(double);
+    const size_t nbk = (size_t)c->n * c->n * sizeof(unsigned);
+    bool ok = cudaMalloc(&p->pos, nb) == cudaSuccess && cudaMalloc(&p->pos2, nb) == cudaSuccess &&
+              cudaMalloc(&p->hist, nb * nsteps) == cudaSuccess &&
+              cudaMalloc(&p->hist2, nb * nsteps) == cudaSuccess &&
+              cudaMalloc(&p->corder, n1 * 8) == cudaSuccess &&
+              cudaMalloc(&p->corder2, n1 * 8) == cudaSuccess &&
+              cudaMalloc(&p->sample, nb) == cudaSuccess &&
+              cudaMalloc(&p->key, n1 * 4) == cudaSuccess &&
+              cudaMalloc(&p->rank, n1 * 4) == cudaSuccess &&
+              cudaMalloc(&p->count, nbk) == cudaSuccess && cudaMalloc(&p->offset, nbk) == cudaSuccess;
+    if (!ok) {
         cudaGetLastError();
         bfg_particles_destroy(p);
         return fail(c, BFG_ENOMEM, "cannot allocate tracer state for %lld tracers", (long long)n);
     }
-    auto cleanup = [&](int code) {
-        bfg_particles_destroy(p);
-        return code;
-    };
-    if (n > 0) {
-        if (cudaMemcpy(p->pos, pos, (size_t)n * 3 * 8, cudaMemcpyHostToDevice) != cudaSuccess)
-            return cleanup(fail(c, BFG_ECUDA, "tracer upload failed"));
-        if (rhs) {
-            if (cudaMemcpy(p->hist, rhs, (size_t)n * 3 * 8 * nsteps, cudaMemcpyHostToDevice) !=
-                cudaSuccess)
-                return cleanup(fail(c, BFG_ECUDA, "tracer upload failed"));
-            bool z = true;
-            for (int64_t i = 0; i < n * 3 && z; ++i) z = rhs[i] == 0.0;
-            p->rhs0_zero = z;
-        } else {
-            cudaMemset(p->hist, 0, (size_t)n * 3 * 8 * nsteps);
-            p->rhs0_zero = true;
-        }
-    }
     p->idx.resize((size_t)n);
-    for (int64_t i = 0; i < n; ++i) p->idx[i] = idx ? idx[i] : i;
+    for (int64_t i = 0; i < n; ++i) {
+        p->idx[i] = idx ? idx[i] : i;
+        if (p->idx[i] != i) p->identity = false;
+    }
+    if (!p->identity) {
+        p->by_index.resize((size_t)n);
+        for (int64_t i = 0; i < n; ++i) p->by_index[i] = i;
+        std::sort(p->by_index.begin(), p->by_index.end(),
+                  [&](int64_t a, int64_t b) { return p->idx[a] < p->idx[b]; });
+    }
     *out = p;
+    rc = bfg_particles_upload(p, pos, rhs, step_idx);
+    if (rc) {
+        *out = nullptr;
+        bfg_particles_destroy(p);
+        return rc;
+    }
     return 0;
 }
 
 void bfg_particles_destroy(bfg_pctx* p) {
     if (!p) return;
     if (p->ctx) cudaSetDevice(p->ctx->device);
-    if (p->pos) cudaFree(p->pos);
-    if (p->hist) cudaFree(p->hist);
-    if (p->sample) cudaFree(p->sample);
+    void* bufs[] = {p->pos, p->pos2, p->hist, p->hist2, p->corder, p->corder2,
+                    p->sample, p->key, p->rank, p->count, p->offset};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
     delete p;
 }
 
@@ -923,19 +1026,6 @@ int bfg_particles_complete_loop(bfg_pctx* p, double dt) {
     return 0;
 }
 
-static int to_index_order(bfg_pctx* p, const std::vector<double>& dev_order, int width,
-                          double* out) {
-    // tracers are kept in creation order; the reference writes them sorted by
-    // global index (abstract_particles_output.hpp:144-265)
-    std::vector<int64_t> order(p->n);
-    for (int64_t i = 0; i < p->n; ++i) order[i] = i;
-    std::sort(order.begin(), order.end(),
-              [&](int64_t a, int64_t b) { return p->idx[a] < p->idx[b]; });
-    for (int64_t k = 0; k < p->n; ++k)
-        for (int d = 0; d < width; ++d) out[k * width + d] = dev_order[order[k] * width + d];
-    return 0;
-}
-
 int bfg_particles_sample_velocity(bfg_pctx* p, double* out) {
     if (!p || !out) return BFG_EINVAL;
     bfg_ctx* c = p->ctx;
@@ -944,39 +1034,32 @@ int bfg_particles_sample_velocity(bfg_pctx* p, double* out) {
     int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, p->sample)
                                 : tracers_dispatch<double>(c, pp, p, p->sample);
     if (rc) return rc;
-    std::vector<double> h((size_t)p->n * 3);
-    CU(cudaMemcpyAsync(h.data(), p->sample, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
-    return to_index_order(p, h, 3, out);
+    return fetch_index_order(p, p->sample, 3, out);
 }
 
 int bfg_particles_download(bfg_pctx* p, double* pos, double* rhs, int64_t* idx) {
     if (!p) return BFG_EINVAL;
     bfg_ctx* c = p->ctx;
     CU(cudaSetDevice(c->device));
-    CU(cudaStreamSynchronize(c->stream));
     const size_t n3 = (size_t)p->n * 3;
-    if (pos) {
-        std::vector<double> h(n3);
-        CU(cudaMemcpy(h.data(), p->pos, n3 * 8, cudaMemcpyDeviceToHost));
-        to_index_order(p, h, 3, pos);
-    }
+    int rc;
+    if (pos && (rc = fetch_index_order(p, p->pos, 3, pos))) return rc;
     if (rhs) {
-        std::vector<double> h(n3);
         for (int j = 0; j < p->nsteps; ++j) {
             if (j == 0 && p->rhs0_zero) {
                 std::fill(rhs, rhs + n3, 0.0);
                 continue;
             }
             const int slot = (p->head + j) % p->nsteps;
-            CU(cudaMemcpy(h.data(), p->hist + (size_t)slot * n3, n3 * 8, cudaMemcpyDeviceToHost));
-            to_index_order(p, h, 3, rhs + (size_t)j * n3);
+            if ((rc = fetch_index_order(p, p->hist + (size_t)slot * n3, 3, rhs + (size_t)j * n3)))
+                return rc;
         }
     }
     if (idx) {
-        std::vector<int64_t> s(p->idx);
-        std::sort(s.begin(), s.end());
-        std::copy(s.begin(), s.end(), idx);
+        if (p->identity)
+            for (int64_t i = 0; i < p->n; ++i) idx[i] = i;
+        else
+            for (int64_t k = 0; k < p->n; ++k) idx[k] = p->idx[p->by_index[k]];
     }
     return 0;
 }
@@ -986,8 +1069,11 @@ int bfg_particles_upload(bfg_pctx* p, const double* pos, const double* rhs, int 
     bfg_ctx* c = p->ctx;
     CU(cudaSetDevice(c->device));
     const size_t n3 = (size_t)p->n * 3;
-    CU(cudaMemcpyAsync(p->pos, pos, n3 * 8, cudaMemcpyHostToDevice, c->stream));
     p->head = 0;
+    p->step_idx = step_idx;
+    if (p->n == 0) return 0;
+    // back to creation order, then cell order
+    CU(cudaMemcpyAsync(p->pos, pos, n3 * 8, cudaMemcpyHostToDevice, c->stream));
     if (rhs) {
         CU(cudaMemcpyAsync(p->hist, rhs, n3 * 8 * p->nsteps, cudaMemcpyHostToDevice, c->stream));
         bool z = true;
@@ -997,7 +1083,10 @@ int bfg_particles_upload(bfg_pctx* p, const double* pos, const double* rhs, int 
         CU(cudaMemsetAsync(p->hist, 0, n3 * 8 * p->nsteps, c->stream));
         p->rhs0_zero = true;
     }
-    p->step_idx = step_idx;
+    iota64<<<(unsigned)((p->n + 255) / 256), 256, 0, c->stream>>>(p->corder, p->n);
+    int rc = after_launch(c, "iota64");
+    if (rc) return rc;
+    if ((rc = tracer_sort(p))) return rc;
     CU(cudaStreamSynchronize(c->stream));
     return 0;
 }

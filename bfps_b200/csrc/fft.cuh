@@ -56,6 +56,43 @@ __device__ __forceinline__ cpx<T> rot90(cpx<T> a) {
     return INV ? mk<T>(-a.y, a.x) : mk<T>(a.y, -a.x);
 }
 
+// ------------------------------------------------------ async copies --
+// cp.async (global -> shared, bypassing registers), PTX ISA 7.0+.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+// copy of VB bytes (16 or 8)
+template <int VB>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+    if constexpr (VB == 16) cp_async16(dst, src);
+    else cp_async8(dst, src);
+}
+template <int VB>
+struct vec_of;
+template <>
+struct vec_of<16> {
+    using type = float4;
+};
+template <>
+struct vec_of<8> {
+    using type = float2;
+};
+
 // ---------------------------------------------------------------- plans --
 __host__ __device__ constexpr int plan_step(int L) {
     return (L % 8 == 0 && L / 8 != 2) ? 8 : ((L % 4 == 0) ? 4 : 2);

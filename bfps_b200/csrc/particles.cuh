@@ -56,6 +56,66 @@ __device__ __forceinline__ void cell_of(double pos, double box, double h, int N,
     *cell = ((lvl % N) + N) % N;
 }
 
+// x-segment of one stencil row: 2n+2 points x 3 components, contiguous in
+// [z][y][x][c] unless the stencil wraps across the periodic x boundary.
+// Loads 16-byte vectors from the aligned-down start and accumulates
+// sum_ix w[ix] * f(ix, c) in double.
+template <typename T, int NB>
+__device__ __forceinline__ void row_accumulate(const T* __restrict__ row, int x0, int N,
+                                               const double* wxc, double& a0, double& a1,
+                                               double& a2) {
+    constexpr int NP = 2 * NB + 2;
+    constexpr int VEC = 16 / (int)sizeof(T);  // elements per 16-byte vector
+    constexpr int NV = (3 * NP + VEC - 1) / VEC + 1;  // vectors covering any alignment
+    if (x0 >= 0 && x0 + NP <= N) {
+        const int e0 = x0 * 3;
+        const int base = e0 & ~(VEC - 1);
+        const int off = e0 - base;
+        T buf[NV * VEC];
+        const int maxv = (N * 3 - base) / VEC;  // vectors left in this row
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            if (v < maxv) {
+                if constexpr (sizeof(T) == 4) {
+                    const float4 q = *reinterpret_cast<const float4*>(row + base + v * VEC);
+                    buf[v * 4 + 0] = q.x; buf[v * 4 + 1] = q.y;
+                    buf[v * 4 + 2] = q.z; buf[v * 4 + 3] = q.w;
+                } else {
+                    const double2 q = *reinterpret_cast<const double2*>(row + base + v * VEC);
+                    buf[v * 2 + 0] = q.x; buf[v * 2 + 1] = q.y;
+                }
+            } else {
+#pragma unroll
+                for (int u = 0; u < VEC; ++u) buf[v * VEC + u] = (T)0;
+            }
+        }
+#pragma unroll
+        for (int ix = 0; ix < NP; ++ix) {
+            T f[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int j = ix * 3 + c;
+                // buf[j + off], off in [0, VEC)
+                T v = buf[j];
+#pragma unroll
+                for (int o = 1; o < VEC; ++o) v = (off == o) ? buf[j + o] : v;
+                f[c] = v;
+            }
+            a0 += (double)f[0] * wxc[ix];
+            a1 += (double)f[1] * wxc[ix];
+            a2 += (double)f[2] * wxc[ix];
+        }
+    } else {
+#pragma unroll
+        for (int ix = 0; ix < NP; ++ix) {
+            const int xx = (x0 + ix + N) % N;
+            a0 += (double)row[xx * 3 + 0] * wxc[ix];
+            a1 += (double)row[xx * 3 + 1] * wxc[ix];
+            a2 += (double)row[xx * 3 + 2] * wxc[ix];
+        }
+    }
+}
+
 template <typename T, int NB, int MM>
 __global__ void __launch_bounds__(128)
 tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ pos,
@@ -78,25 +138,20 @@ tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ p
 
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
     const size_t rowN = (size_t)N;
+    const int x0 = g[0] - NB;
 #pragma unroll 1
     for (int iz = 0; iz < NP; ++iz) {
-        int z = g[2] - NB + iz;
-        z = (z + N) % N;
+        const int z = (g[2] - NB + iz + N) % N;
+#pragma unroll 1
+        for (int iy = 0; iy < NP; ++iy) {
+            const int y = (g[1] - NB + iy + N) % N;
+            // coefficient (bz * by) * bx of apply_computation
+            const double bzy = wz[iz] * wy[iy];
+            double wxc[NP];
 #pragma unroll
-        for (int ix = 0; ix < NP; ++ix) {
-            int xx = g[0] - NB + ix;
-            xx = (xx + N) % N;
-            const double bzx = wz[iz];
-#pragma unroll
-            for (int iy = 0; iy < NP; ++iy) {
-                int y = g[1] - NB + iy;
-                y = (y + N) % N;
-                const double coef = (bzx * wy[iy]) * wx[ix];
-                const T* f = ru + (((size_t)z * rowN + y) * rowN + xx) * 3;
-                acc0 += (double)f[0] * coef;
-                acc1 += (double)f[1] * coef;
-                acc2 += (double)f[2] * coef;
-            }
+            for (int ix = 0; ix < NP; ++ix) wxc[ix] = bzy * wx[ix];
+            row_accumulate<T, NB>(ru + ((size_t)z * rowN + y) * rowN * 3, x0, N, wxc, acc0, acc1,
+                                  acc2);
         }
     }
     if (!pp.move) {
@@ -146,6 +201,69 @@ tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ p
         }
         pos[i * 3 + d] = x;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Cell ordering of the tracers (counting sort on the (z, y) cell row).
+// The single-rank reference reorders its arrays by z-layer in every
+// redistribute (particles_distr_mpi.hpp:798-831); here the order only serves
+// memory locality of the gather (every result is per tracer), so the arrays
+// are re-sorted every few steps.  Order inside a bucket is not fixed.
+__global__ void tracer_keys(const PParams pp, const double* __restrict__ pos,
+                            unsigned* __restrict__ key, unsigned* __restrict__ rank,
+                            unsigned* __restrict__ count) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pp.n) return;
+    const int N = pp.N;
+    int gz, gy;
+    double fr;
+    cell_of(pos[i * 3 + 2], pp.box[2], pp.hstep[2], N, &gz, &fr);
+    cell_of(pos[i * 3 + 1], pp.box[1], pp.hstep[1], N, &gy, &fr);
+    const unsigned k = (unsigned)gz * (unsigned)N + (unsigned)gy;
+    key[i] = k;
+    rank[i] = atomicAdd(&count[k], 1u);
+}
+
+// exclusive scan of nb counts with one CTA of 1024 threads
+__global__ void __launch_bounds__(1024) bucket_scan(const unsigned* __restrict__ count,
+                                                    unsigned* __restrict__ offset, int nb) {
+    __shared__ unsigned part[1024];
+    const int t = threadIdx.x;
+    const int per = (nb + 1023) / 1024;
+    const int b0 = t * per, b1 = min(nb, b0 + per);
+    unsigned s = 0;
+    for (int b = b0; b < b1; ++b) s += count[b];
+    part[t] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const unsigned v = t >= o ? part[t - o] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    unsigned run = part[t] - s;  // exclusive prefix of this thread's range
+    for (int b = b0; b < b1; ++b) {
+        offset[b] = run;
+        run += count[b];
+    }
+}
+
+__global__ void tracer_scatter(const PParams pp, const unsigned* __restrict__ key,
+                               const unsigned* __restrict__ rank,
+                               const unsigned* __restrict__ offset,
+                               const double* __restrict__ pos, const double* __restrict__ hist,
+                               const int64_t* __restrict__ idx, double* __restrict__ pos2,
+                               double* __restrict__ hist2, int64_t* __restrict__ idx2) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pp.n) return;
+    const int64_t d = (int64_t)offset[key[i]] + rank[i];
+    const size_t slot = (size_t)pp.n * 3;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) pos2[d * 3 + c] = pos[i * 3 + c];
+    for (int s = 0; s < pp.nsteps; ++s)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) hist2[s * slot + d * 3 + c] = hist[s * slot + i * 3 + c];
+    idx2[d] = idx[i];
 }
 
 }  // namespace bfg

@@ -61,22 +61,39 @@ __host__ __device__ constexpr bool col_inverse(int mode) {
 __host__ __device__ constexpr int pow2floor(int v) {
     return v < 2 ? 1 : 2 * pow2floor(v / 2);
 }
-// kx columns per CTA: keep the tile near 96 KB (two CTAs per SM)
+constexpr int COL_THREADS = 512;
+constexpr int SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per CTA we plan for
+
+// tile row pitch (complex) for a tile of TKX kx columns: keeps every row
+// 16-byte aligned and breaks the worst bank patterns
+template <typename T, int NB>
+__host__ __device__ constexpr int col_pitch_for(int tkx) {
+    return NB * 3 * tkx + (sizeof(T) == 4 ? 2 : 1);
+}
+template <typename T, int N, int NB>
+__host__ __device__ constexpr size_t col_bytes_for(int tkx) {
+    return (size_t)(2 * N * col_pitch_for<T, NB>(tkx) + N) * sizeof(cpx<T>);
+}
+// kx columns per tile: the widest power of two (<= 16) whose two tile
+// buffers fit the shared-memory budget
+template <typename T, int N, int NB>
+__host__ __device__ constexpr int col_tkx_from(int tkx) {
+    return (tkx <= 1 || col_bytes_for<T, N, NB>(tkx) <= (size_t)SMEM_BUDGET)
+               ? tkx
+               : col_tkx_from<T, N, NB>(tkx / 2);
+}
 template <typename T, int N, int NB>
 __host__ __device__ constexpr int col_tkx() {
-    return pow2floor(98304 / (N * NB * 3 * (int)sizeof(cpx<T>))) > 16
-               ? 16
-               : pow2floor(98304 / (N * NB * 3 * (int)sizeof(cpx<T>)));
+    return col_tkx_from<T, N, NB>(16);
 }
 template <typename T, int N, int MODE>
-__host__ __device__ constexpr int col_pitch() {  // complex per tile row
-    return col_nb(MODE) * 3 * col_tkx<T, N, col_nb(MODE)>() + 1;
+__host__ __device__ constexpr int col_pitch() {
+    return col_pitch_for<T, col_nb(MODE)>(col_tkx<T, N, col_nb(MODE)>());
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t col_smem_bytes() {
-    return (size_t)(N * col_pitch<T, N, MODE>() + N) * sizeof(cpx<T>);
+    return col_bytes_for<T, N, col_nb(MODE)>(col_tkx<T, N, col_nb(MODE)>());
 }
-constexpr int COL_THREADS = 256;
 
 template <int N>
 __device__ __forceinline__ double kwrap(int i, double dk) {
@@ -104,232 +121,295 @@ __device__ __forceinline__ void divfree(A kx, A ky, A kz, A inv_k2, cpx<A>* a) {
 template <typename T>
 __device__ __forceinline__ cpx<T> zero_c() { return mk<T>((T)0, (T)0); }
 
+// global row of tile row l (input side) / lo (output side) for a pass mode
+template <int N, int MODE>
+__device__ __forceinline__ size_t col_in_row(int a, int l) {
+    if (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) return (size_t)a * N + l;  // S[ky=a][kz=l]
+    if (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN) return (size_t)l * N + a;                   // W[z=l][ky=a]
+    return (size_t)a * N + l;                                                                // W[z=a][y=l]
+}
+template <int N, int MODE>
+__device__ __forceinline__ size_t col_out_row(int a, int lo) {
+    if (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) return (size_t)lo * N + a;  // W[z=lo][ky=a]
+    return (size_t)a * N + lo;                                                                 // S or W[z=a]
+}
+
 // ---------------------------------------------------------------------------
-// Strided-axis pass.  grid = (kx tiles, N): blockIdx.y is the fixed outer
-// index a, the transform runs along l over N rows of the tile.
+// Strided-axis pass.  Persistent CTAs (grid = SMs) walk the tiles
+// t = (a, kx-tile), kx-tile fastest; each tile (N rows x TKX kx columns x
+// 3 components x NB buffers) is streamed into one of two shared-memory
+// buffers with cp.async while the previous tile is transformed along l.
 // fac: per-axis integrating-factor tables, 3 factors x (NXV + N + N):
 //      [f][0..NXV) kx, [f][NXV..NXV+N) ky, [f][NXV+N..NXV+2N) kz, where
 //      f = 0: exp(-nu k^2 dt), 1: exp(-nu k^2 dt/2), 2: exp(+nu k^2 dt/2)
 //      per axis (their product over the axes is the factor of k^2).
 template <typename T, int N, int MODE>
-__global__ void __launch_bounds__(COL_THREADS)
+__device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
+                                               const cpx<T>* in1, int a, int kx0, int ncol,
+                                               size_t nxp3, int tid) {
+    constexpr int NB = col_nb(MODE);
+    constexpr int NBIN = col_nbin(MODE);
+    constexpr int TKX = col_tkx<T, N, NB>();
+    constexpr int W = 3 * TKX;
+    constexpr int PR = col_pitch<T, N, MODE>();
+    constexpr int VB = ((W * (int)sizeof(cpx<T>)) % 16 == 0) ? 16 : 8;
+    constexpr int VPE = VB / (int)sizeof(cpx<T>) > 0 ? VB / (int)sizeof(cpx<T>) : 1;  // complex per copy
+    constexpr int WV = W / VPE;
+    const int nvalid = (3 * ncol + VPE - 1) / VPE;
+    for (int e = tid; e < N * NBIN * WV; e += COL_THREADS) {
+        const int v = e % WV;
+        const int r = e / WV;
+        const int b = r % NBIN;
+        const int l = r / NBIN;
+        if (v >= nvalid) continue;
+        const cpx<T>* src = ((b == 0) ? in0 : in1) + col_in_row<N, MODE>(a, l) * nxp3 +
+                            (size_t)kx0 * 3 + v * VPE;
+        const int bdst = (MODE == CM_IZ_VEL) ? 1 : b;  // w^ goes to slot 1
+        cp_async<VB>(&tile[l * PR + bdst * W + v * VPE], src);
+    }
+}
+
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(COL_THREADS, 1)
 col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restrict__ in1,
          cpx<T>* out0, cpx<T>* out1, const cpx<T>* __restrict__ rk_v0,
          const cpx<T>* __restrict__ rk_vp, const cpx<T>* __restrict__ fsrc,
          const T* __restrict__ filt, const T* __restrict__ fac,
-         const cpx<T>* __restrict__ tw_g) {
+         const cpx<T>* __restrict__ tw_g, int ntx, int ntiles) {
     constexpr int NB = col_nb(MODE);
-    constexpr int NBIN = col_nbin(MODE);
     constexpr int TKX = col_tkx<T, N, NB>();
     constexpr int W = 3 * TKX;                     // complex per row per buffer
     constexpr int PR = col_pitch<T, N, MODE>();    // tile row pitch
+    constexpr int TILE = N * PR;
     constexpr bool INV = col_inverse(MODE);
+    constexpr int VB = ((W * (int)sizeof(cpx<T>)) % 16 == 0) ? 16 : 8;
+    constexpr int VPE = VB / (int)sizeof(cpx<T>) > 0 ? VB / (int)sizeof(cpx<T>) : 1;
+    constexpr int WV = W / VPE;
+    using V = typename vec_of<VB>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cpx<T>* tile = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* tw = tile + N * PR;
+    cpx<T>* bufs = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* tw = bufs + 2 * TILE;
 
     const int tid = threadIdx.x;
-    const int a = blockIdx.y;
-    const int kx0 = blockIdx.x * TKX;
-    const int ncol = min(TKX, kp.nxv - kx0);
     const size_t nxp3 = (size_t)kp.nxp * 3;
-
     for (int i = tid; i < N; i += COL_THREADS) tw[i] = tw_g[i];
 
-    // ---- load (rows l, buffers b, complex q) ---------------------------
-    for (int e = tid; e < N * NBIN * W; e += COL_THREADS) {
-        const int q = e % W;
-        const int r = e / W;
-        const int b = r % NBIN;
-        const int l = r / NBIN;
-        size_t row;
-        if (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U)
-            row = (size_t)a * N + l;                                             // S[ky=a][kz=l]
-        else if (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN) row = (size_t)l * N + a;  // W[z=l][ky=a]
-        else row = (size_t)a * N + l;                                            // W[z=a][y=l]
-        const cpx<T>* src = (b == 0) ? in0 : in1;
-        cpx<T> v = zero_c<T>();
-        if (q < 3 * ncol) v = src[row * nxp3 + (size_t)kx0 * 3 + q];
-        const int bdst = (MODE == CM_IZ_VEL) ? 1 : b;  // w^ goes to slot 1
-        tile[l * PR + bdst * W + q] = v;
+    int t = blockIdx.x;
+    if (t < ntiles) {
+        const int kx0 = (t % ntx) * TKX;
+        col_issue_load<T, N, MODE>(bufs, in0, in1, t / ntx, kx0, min(TKX, kp.nxv - kx0), nxp3, tid);
     }
-    __syncthreads();
-
-    // ---- prologue: u^ = i k x w^ / k^2 for 0 < k^2 <= kM^2 ---------------
-    if constexpr (MODE == CM_IZ_VEL || MODE == CM_IZ_U) {
-        constexpr int WSRC = (MODE == CM_IZ_VEL) ? W : 0;  // slot holding w^
-        const double ky = kwrap<N>(a, kp.dky);
-        for (int e = tid; e < N * TKX; e += COL_THREADS) {
-            const int col = e % TKX;
-            const int l = e / TKX;
-            const double kz = kwrap<N>(l, kp.dkz);
-            const double kx = (double)(kx0 + col) * kp.dkx;
-            const double k2 = (kx * kx + ky * ky) + kz * kz;
-            cpx<T>* w = &tile[l * PR + WSRC + col * 3];
-            cpx<T> u[3];
-            if (k2 <= kp.kM2 && k2 > 0.0) {
-                const T ik2 = (T)(1.0 / k2);
-                cpx<T> wv[3] = {w[0], w[1], w[2]};
-                curl<T>((T)kx, (T)ky, (T)kz, wv, u);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) u[c] = scale(u[c], ik2);
-            } else {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) u[c] = zero_c<T>();
+    cp_async_commit();
+    for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
+        cpx<T>* tile = bufs + (it & 1) * TILE;
+        {
+            const int tn = t + gridDim.x;
+            if (tn < ntiles) {
+                const int kx0n = (tn % ntx) * TKX;
+                col_issue_load<T, N, MODE>(bufs + ((it + 1) & 1) * TILE, in0, in1, tn / ntx, kx0n,
+                                           min(TKX, kp.nxv - kx0n), nxp3, tid);
             }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) tile[l * PR + col * 3 + c] = u[c];
+            cp_async_commit();
         }
+        cp_async_wait<1>();
         __syncthreads();
-    }
+        const int a = t / ntx;
+        const int kx0 = (t % ntx) * TKX;
+        const int ncol = min(TKX, kp.nxv - kx0);
 
-    // ---- FFT along l: NB*W pencils, pencil stride 1, element stride PR ----
-    dif<T, N, INV, NB * W, 1, PR, true, N>(tile, tw, tid, COL_THREADS);
-
-    // ---- epilogue ------------------------------------------------------
-    if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
-        const double ky = kwrap<N>(a, kp.dky);
-        const int nxv = kp.nxv;
-        for (int e = tid; e < N * TKX; e += COL_THREADS) {
-            const int col = e % TKX;
-            const int l = e / TKX;  // output kz index
-            if (col >= ncol) continue;
-            const int ix = kx0 + col;
-            const double kz = kwrap<N>(l, kp.dkz);
-            const double kx = (double)ix * kp.dkx;
-            const double k2 = (kx * kx + ky * ky) + kz * kz;
-            const int p = dif_position<N>(l);
-            cpx<T> nl[3];
+        // ---- prologue: u^ = i k x w^ / k^2 for 0 < k^2 <= kM^2 -----------
+        if constexpr (MODE == CM_IZ_VEL || MODE == CM_IZ_U) {
+            constexpr int WSRC = (MODE == CM_IZ_VEL) ? W : 0;  // slot holding w^
+            const double ky = kwrap<N>(a, kp.dky);
+            for (int e = tid; e < N * TKX; e += COL_THREADS) {
+                const int col = e % TKX;
+                const int l = e / TKX;
+                const double kz = kwrap<N>(l, kp.dkz);
+                const double kx = (double)(kx0 + col) * kp.dkx;
+                const double k2 = (kx * kx + ky * ky) + kz * kz;
+                cpx<T>* w = &tile[l * PR + WSRC + col * 3];
+                cpx<T> u[3];
+                if (k2 <= kp.kM2 && k2 > 0.0) {
+                    const T ik2 = (T)(1.0 / k2);
+                    cpx<T> wv[3] = {w[0], w[1], w[2]};
+                    curl<T>((T)kx, (T)ky, (T)kz, wv, u);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) nl[c] = tile[p * PR + col * 3 + c];
-            // dealias (kspace.cpp:461-485)
-            if (kp.dealias == 1) {
-                int key = (int)rint(k2 * kp.inv_dk2);
-                key = key < kp.nfilt ? key : kp.nfilt - 1;
-                const T f = filt[key];
+                    for (int c = 0; c < 3; ++c) u[c] = scale(u[c], ik2);
+                } else {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) nl[c] = scale(nl[c], f);
-            } else if (k2 >= kp.kM2) {
+                    for (int c = 0; c < 3; ++c) u[c] = zero_c<T>();
+                }
 #pragma unroll
-                for (int c = 0; c < 3; ++c) nl[c] = zero_c<T>();
+                for (int c = 0; c < 3; ++c) tile[l * PR + col * 3 + c] = u[c];
             }
-            // i k x (vorticity_equation.cpp:323-350)
-            cpx<T> t[3];
-            curl<T>((T)kx, (T)ky, (T)kz, nl, t);
-            const size_t pt = ((size_t)a * N + l) * kp.nxp + ix;  // S[ky=a][kz=l][kx]
-            // forcing (vorticity_equation.cpp:241-288), factor 1
-            if (kp.forcing == 1) {
-                const double kn = sqrt(k2);
-                if (kp.fk0 <= kn && kp.fk1 >= kn) {
+            __syncthreads();
+        }
+
+        // ---- FFT along l: NB*W pencils, pencil stride 1, element stride PR --
+        dif<T, N, INV, NB * W, 1, PR, true, N>(tile, tw, tid, COL_THREADS);
+
+        // ---- epilogue ----------------------------------------------------
+        if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
+            const double ky = kwrap<N>(a, kp.dky);
+            const int nxv = kp.nxv;
+            for (int e = tid; e < N * TKX; e += COL_THREADS) {
+                const int col = e % TKX;
+                const int l = e / TKX;  // output kz index
+                if (col >= ncol) continue;
+                const int ix = kx0 + col;
+                const size_t pt = ((size_t)a * N + l) * kp.nxp + ix;  // S[ky=a][kz=l][kx]
+                // RK operands first, so their latency overlaps the k-space math
+                cpx<T> v0[3], vp[3];
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const cpx<T> fv = fsrc[pt * 3 + c];
-                        t[c].x += (T)(kp.famp * (double)fv.x);
-                        t[c].y += (T)(kp.famp * (double)fv.y);
+                for (int c = 0; c < 3; ++c) v0[c] = rk_v0[pt * 3 + c];
+                if (MODE != CM_FZ_RK1) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) vp[c] = rk_vp[pt * 3 + c];
+                }
+                const double kz = kwrap<N>(l, kp.dkz);
+                const double kx = (double)ix * kp.dkx;
+                const double k2 = (kx * kx + ky * ky) + kz * kz;
+                const int p = dif_position<N>(l);
+                cpx<T> nl[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) nl[c] = tile[p * PR + col * 3 + c];
+                // dealias (kspace.cpp:461-485)
+                if (kp.dealias == 1) {
+                    int key = (int)rint(k2 * kp.inv_dk2);
+                    key = key < kp.nfilt ? key : kp.nfilt - 1;
+                    const T f = filt[key];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) nl[c] = scale(nl[c], f);
+                } else if (k2 >= kp.kM2) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) nl[c] = zero_c<T>();
+                }
+                // i k x (vorticity_equation.cpp:323-350)
+                cpx<T> tt[3];
+                curl<T>((T)kx, (T)ky, (T)kz, nl, tt);
+                // forcing (vorticity_equation.cpp:241-288), factor 1
+                if (kp.forcing == 1) {
+                    const double kn = sqrt(k2);
+                    if (kp.fk0 <= kn && kp.fk1 >= kn) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const cpx<T> fv = fsrc[pt * 3 + c];
+                            tt[c].x += (T)(kp.famp * (double)fv.x);
+                            tt[c].y += (T)(kp.famp * (double)fv.y);
+                        }
+                    }
+                } else if (kp.forcing == 2) {
+                    if (ix == 0 && l == 0) {
+                        if (a == kp.fmode) tt[2].x -= (T)(kp.famp / 2);
+                        if (a == N - kp.fmode) tt[2].x -= (T)(kp.famp / 2);
                     }
                 }
-            } else if (kp.forcing == 2) {
-                if (ix == 0 && l == 0) {
-                    if (a == kp.fmode) t[2].x -= (T)(kp.famp / 2);
-                    if (a == N - kp.fmode) t[2].x -= (T)(kp.famp / 2);
-                }
-            }
-            // force_divfree on the nonlinear term; zero mode cleared
-            const bool kzero = (a == 0 && l == 0 && ix == 0);
-            if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), t);
-            if (kzero) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) t[c] = zero_c<T>();
-            }
-            // RK update (vorticity_equation.cpp:366-434), only for k2 <= kM2
-            const bool inside = k2 <= kp.kM2;
-            const T dt = (T)kp.dt;
-            cpx<T> o[3];
-            const int nfac = nxv + 2 * N;
-            if (MODE == CM_FZ_RK1) {
-                const T f0 = fac[ix] * fac[nxv + a] * fac[nxv + N + l];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const cpx<T> v0 = rk_v0[pt * 3 + c];
-                    o[c] = inside ? mk<T>((v0.x + dt * t[c].x) * f0, (v0.y + dt * t[c].y) * f0)
-                                  : zero_c<T>();
-                }
-            } else if (MODE == CM_FZ_RK2) {
-                const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
-                const T f1 = fac[2 * nfac + ix] * fac[2 * nfac + nxv + a] *
-                             fac[2 * nfac + nxv + N + l];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const cpx<T> v0 = rk_v0[pt * 3 + c];
-                    const cpx<T> v1 = rk_vp[pt * 3 + c];
-                    o[c] = inside ? mk<T>((3 * v0.x * f0 + (v1.x + dt * t[c].x) * f1) * (T)0.25,
-                                          (3 * v0.y * f0 + (v1.y + dt * t[c].y) * f1) * (T)0.25)
-                                  : zero_c<T>();
-                }
-            } else {
-                const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const cpx<T> v0 = rk_v0[pt * 3 + c];
-                    const cpx<T> v2 = rk_vp[pt * 3 + c];
-                    o[c] = inside ? mk<T>((v0.x * f0 + 2 * (v2.x + dt * t[c].x)) * f0 / (T)3,
-                                          (v0.y * f0 + 2 * (v2.y + dt * t[c].y)) * f0 / (T)3)
-                                  : v0;
-                }
-                // final force_divfree of the state (vorticity_equation.cpp:436)
-                if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), o);
+                // force_divfree on the nonlinear term; zero mode cleared
+                const bool kzero = (a == 0 && l == 0 && ix == 0);
+                if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), tt);
                 if (kzero) {
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
+                    for (int c = 0; c < 3; ++c) tt[c] = zero_c<T>();
+                }
+                // RK update (vorticity_equation.cpp:366-434), only for k2 <= kM2
+                const bool inside = k2 <= kp.kM2;
+                const T dt = (T)kp.dt;
+                cpx<T> o[3];
+                const int nfac = nxv + 2 * N;
+                if (MODE == CM_FZ_RK1) {
+                    const T f0 = fac[ix] * fac[nxv + a] * fac[nxv + N + l];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        o[c] = inside ? mk<T>((v0[c].x + dt * tt[c].x) * f0,
+                                              (v0[c].y + dt * tt[c].y) * f0)
+                                      : zero_c<T>();
+                } else if (MODE == CM_FZ_RK2) {
+                    const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
+                    const T f1 = fac[2 * nfac + ix] * fac[2 * nfac + nxv + a] *
+                                 fac[2 * nfac + nxv + N + l];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        o[c] = inside
+                                   ? mk<T>((3 * v0[c].x * f0 + (vp[c].x + dt * tt[c].x) * f1) * (T)0.25,
+                                           (3 * v0[c].y * f0 + (vp[c].y + dt * tt[c].y) * f1) * (T)0.25)
+                                   : zero_c<T>();
+                } else {
+                    const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        o[c] = inside ? mk<T>((v0[c].x * f0 + 2 * (vp[c].x + dt * tt[c].x)) * f0 / (T)3,
+                                              (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 / (T)3)
+                                      : v0[c];
+                    // final force_divfree of the state (vorticity_equation.cpp:436)
+                    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), o);
+                    if (kzero) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) out0[pt * 3 + c] = o[c];
+            }
+        } else {
+            // plain store of NB buffers, output row lo (natural order); whole
+            // vectors inside the valid columns, single complex at the edge
+            const int nval = 3 * ncol;
+            for (int e = tid; e < N * NB * WV; e += COL_THREADS) {
+                const int v = e % WV;
+                const int r = e / WV;
+                const int b = r % NB;
+                const int lo = r / NB;
+                const int q = v * VPE;
+                if (q >= nval) continue;
+                const size_t row = col_out_row<N, MODE>(a, lo);
+                const int p = dif_position<N>(lo);
+                cpx<T>* dst = ((b == 0) ? out0 : out1) + row * nxp3 + (size_t)kx0 * 3 + q;
+                const cpx<T>* sp = &tile[p * PR + b * W + q];
+                if (q + VPE <= nval) {
+                    *reinterpret_cast<V*>(dst) = *reinterpret_cast<const V*>(sp);
+                } else {
+                    for (int u = 0; u < nval - q; ++u) dst[u] = sp[u];
                 }
             }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) out0[pt * 3 + c] = o[c];
         }
-    } else {
-        // plain store of NB buffers, output row index lo (natural order)
-        for (int e = tid; e < N * NB * W; e += COL_THREADS) {
-            const int q = e % W;
-            const int r = e / W;
-            const int b = r % NB;
-            const int lo = r / NB;
-            if (q >= 3 * ncol) continue;
-            size_t row;
-            if (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U)
-                row = (size_t)lo * N + a;                                            // W[z=lo][ky=a]
-            else if (MODE == CM_FZ_PLAIN) row = (size_t)a * N + lo;                  // S[ky=a][kz=lo]
-            else row = (size_t)a * N + lo;                                           // W[z=a][y=lo]
-            const int p = dif_position<N>(lo);
-            cpx<T>* dst = (b == 0) ? out0 : out1;
-            dst[row * nxp3 + (size_t)kx0 * 3 + q] = tile[p * PR + b * W + q];
-        }
+        __syncthreads();  // this buffer is refilled by the load issued next iteration
     }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
-// Row pass over (z, y) rows of W.  Shared memory: pencils of length
-// PL = N/2 + 1 (+1 pad), buffer-major: pencil (b*3*ROWS + r*3 + c).
 enum RowMode {
     RM_NONLIN = 0,     // (u^, w^) rows -> R2C(u x w / N^3) into out, opt. real u
     RM_C2R = 1,        // complex rows -> real rows
     RM_R2C = 2,        // real rows -> complex rows
 };
-constexpr int ROW_THREADS = 256;
+constexpr int ROW_THREADS = 512;
 
-template <typename T, int N>
-__host__ __device__ constexpr int row_rows() {
-    // about 64 KB of pencils, and at least ~2 CTAs per SM of work
-    return (pow2floor(65536 / (6 * (N / 2 + 2) * (int)sizeof(cpx<T>))) <
-            pow2floor(N * N / 296 > 0 ? N * N / 296 : 1))
-               ? pow2floor(65536 / (6 * (N / 2 + 2) * (int)sizeof(cpx<T>)))
-               : pow2floor(N * N / 296 > 0 ? N * N / 296 : 1);
-}
 template <int N>
 __host__ __device__ constexpr int row_pl() { return N / 2 + 2; }
+template <int N>
+__host__ __device__ constexpr int row_rl() { return (N / 2 + 4) * 3; }  // padded row, complex
+// staging (2 buffers) + pencils + twiddles for R rows
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr size_t row_bytes_for(int R) {
+    return (size_t)((MODE == RM_R2C) ? 2 * R * (N * 3 / 2)             // real rows, as complex pairs
+                                     : 2 * R * (MODE == RM_NONLIN ? 2 : 1) * row_rl<N>()) *
+               sizeof(cpx<T>) +
+           (size_t)((MODE == RM_NONLIN ? 6 : 3) * R * row_pl<N>() + N) * sizeof(cpx<T>);
+}
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr int row_rows_from(int R) {
+    return (R <= 1 || (row_bytes_for<T, N, MODE>(R) <= (size_t)SMEM_BUDGET && R <= (N * N) / 296))
+               ? (R < 1 ? 1 : R)
+               : row_rows_from<T, N, MODE>(R / 2);
+}
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr int row_rows() {
+    return row_rows_from<T, N, MODE>(16);
+}
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t row_smem_bytes() {
-    return (size_t)((MODE == RM_NONLIN ? 6 : 3) * row_rows<T, N>() * row_pl<N>() + N) *
-           sizeof(cpx<T>);
+    return row_bytes_for<T, N, MODE>(row_rows<T, N, MODE>());
 }
 
 // C2R pre-processing of one pencil (k, M-k pairs), X[0], X[M] real parts.
@@ -385,106 +465,158 @@ __device__ __forceinline__ void r2c_post(cpx<T>* s, const cpx<T>* tw, int k) {
     }
 }
 
+// Row pass over (z, y) rows of W.  Persistent CTAs walk tiles of ROWS
+// consecutive rows; each tile's rows are contiguous in HBM and are streamed
+// with cp.async into a staging buffer (two, alternating) while the previous
+// tile is transformed.  Pencils (b*3*ROWS + r*3 + c) of length PL = N/2+2
+// hold the transposed rows for the FFTs.
+template <typename T, int N, int MODE>
+__device__ __forceinline__ void row_issue_load(cpx<T>* stage, const cpx<T>* wu, const cpx<T>* ww,
+                                               const T* rin, size_t row0, size_t nxp3, int tid) {
+    constexpr int ROWS = row_rows<T, N, MODE>();
+    constexpr int VPE = 16 / (int)sizeof(cpx<T>);
+    if constexpr (MODE == RM_R2C) {
+        constexpr int NV = ROWS * N * 3 / 2 / VPE;  // 16-byte vectors of the real rows
+        const cpx<T>* src = reinterpret_cast<const cpx<T>*>(rin + row0 * N * 3);
+        for (int v = tid; v < NV; v += ROW_THREADS) cp_async16(&stage[v * VPE], &src[v * VPE]);
+    } else {
+        constexpr int NBIN = (MODE == RM_NONLIN) ? 2 : 1;
+        constexpr int RL = row_rl<N>();
+        constexpr int NV = ROWS * RL / VPE;  // per buffer
+        for (int e = tid; e < NBIN * NV; e += ROW_THREADS) {
+            const int v = e % NV;
+            const int b = e / NV;
+            const cpx<T>* src = ((b == 0) ? wu : ww) + row0 * nxp3;
+            cp_async16(&stage[b * ROWS * RL + v * VPE], &src[v * VPE]);
+        }
+    }
+}
+
 template <typename T, int N, int MODE, bool WRITE_RU>
-__global__ void __launch_bounds__(ROW_THREADS)
+__global__ void __launch_bounds__(ROW_THREADS, 1)
 row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restrict__ ww,
          cpx<T>* wout, T* __restrict__ rout, const T* __restrict__ rin,
-         const cpx<T>* __restrict__ tw_g) {
+         const cpx<T>* __restrict__ tw_g, int ntiles) {
     constexpr int M = N / 2;
-    constexpr int ROWS = row_rows<T, N>();
+    constexpr int ROWS = row_rows<T, N, MODE>();
     constexpr int PL = row_pl<N>();
+    constexpr int RL = row_rl<N>();
     constexpr int NBIN = (MODE == RM_NONLIN) ? 2 : 1;
+    constexpr int STAGE = (MODE == RM_R2C) ? ROWS * N * 3 / 2 : ROWS * NBIN * RL;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cpx<T>* S = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* stage0 = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* S = stage0 + 2 * STAGE;
     cpx<T>* tw = S + (MODE == RM_NONLIN ? 6 : 3) * ROWS * PL;
     const int tid = threadIdx.x;
-    const size_t row0 = (size_t)blockIdx.x * ROWS;
     const int nxv = kp.nxv;
     const size_t nxp3 = (size_t)kp.nxp * 3;
 
     for (int i = tid; i < N; i += ROW_THREADS) tw[i] = tw_g[i];
 
-    if constexpr (MODE == RM_R2C) {
-        // real rows into digit-reversed complex pencils z[n] = (x[2n], x[2n+1])
-        for (int e = tid; e < ROWS * 3 * M; e += ROW_THREADS) {
-            const int c = e % 3;
-            const int r2 = e / 3;
-            const int n = r2 % M;
-            const int r = r2 / M;
-            const T* src = rin + ((row0 + r) * N + 2 * n) * 3 + c;
-            S[(r * 3 + c) * PL + dif_position<M>(n)] = mk<T>(src[0], src[3]);
+    int t = blockIdx.x;
+    if (t < ntiles) row_issue_load<T, N, MODE>(stage0, wu, ww, rin, (size_t)t * ROWS, nxp3, tid);
+    cp_async_commit();
+    for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
+        const cpx<T>* stage = stage0 + (it & 1) * STAGE;
+        {
+            const int tn = t + gridDim.x;
+            if (tn < ntiles)
+                row_issue_load<T, N, MODE>(stage0 + ((it + 1) & 1) * STAGE, wu, ww, rin,
+                                           (size_t)tn * ROWS, nxp3, tid);
+            cp_async_commit();
         }
+        cp_async_wait<1>();
         __syncthreads();
-    } else {
-        for (int e = tid; e < ROWS * NBIN * nxv * 3; e += ROW_THREADS) {
-            const int q = e % (nxv * 3);
-            const int r2 = e / (nxv * 3);
-            const int b = r2 % NBIN;
-            const int r = r2 / NBIN;
-            const cpx<T>* src = (b == 0) ? wu : ww;
-            const int kx = q / 3, c = q % 3;
-            S[(b * 3 * ROWS + r * 3 + c) * PL + kx] = src[(row0 + r) * nxp3 + q];
-        }
-        __syncthreads();
-        constexpr int NP = NBIN * 3 * ROWS;
-        for (int e = tid; e < NP * (M / 2 + 1); e += ROW_THREADS) {
-            const int k = e % (M / 2 + 1);
-            const int p = e / (M / 2 + 1);
-            c2r_pre<T, N>(S + p * PL, tw, k);
-        }
-        __syncthreads();
-        dif<T, M, true, NP, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
+        const size_t row0 = (size_t)t * ROWS;
 
-        if constexpr (MODE == RM_C2R || WRITE_RU) {
-            // real u (first 3*ROWS pencils) to rout, natural x order
-            for (int e = tid; e < ROWS * N * 3; e += ROW_THREADS) {
+        if constexpr (MODE == RM_R2C) {
+            // real rows into digit-reversed complex pencils z[n] = (x[2n], x[2n+1])
+            const T* rs = reinterpret_cast<const T*>(stage);
+            for (int e = tid; e < ROWS * 3 * M; e += ROW_THREADS) {
                 const int c = e % 3;
                 const int r2 = e / 3;
-                const int x = r2 % N;
-                const int r = r2 / N;
-                const cpx<T> z = S[(r * 3 + c) * PL + dif_position<M>(x >> 1)];
-                rout[((row0 + r) * N + x) * 3 + c] = (x & 1) ? z.y : z.x;
-            }
-            if constexpr (MODE == RM_C2R) return;
-            __syncthreads();
-        }
-        if constexpr (MODE == RM_NONLIN) {
-            // u x w / npoints at each position (two grid points per position)
-            const T inv_np = (T)1 / ((T)N * (T)N * (T)N);
-            for (int e = tid; e < ROWS * M; e += ROW_THREADS) {
-                const int p = e % M;
-                const int r = e / M;
-                cpx<T> u[3], w[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    u[c] = S[(r * 3 + c) * PL + p];
-                    w[c] = S[(3 * ROWS + r * 3 + c) * PL + p];
-                }
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc) {
-                    const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
-                    const T tx = u[c1].x * w[c2].x - u[c2].x * w[c1].x;
-                    const T ty = u[c1].y * w[c2].y - u[c2].y * w[c1].y;
-                    S[(r * 3 + cc) * PL + p] = mk<T>(tx * inv_np, ty * inv_np);
-                }
+                const int n = r2 % M;
+                const int r = r2 / M;
+                const T* src = rs + ((size_t)r * N + 2 * n) * 3 + c;
+                S[(r * 3 + c) * PL + dif_position<M>(n)] = mk<T>(src[0], src[3]);
             }
             __syncthreads();
+        } else {
+            // transpose [r][kx][c] -> pencils [b][r][c][kx]
+            for (int e = tid; e < ROWS * NBIN * nxv * 3; e += ROW_THREADS) {
+                const int q = e % (nxv * 3);
+                const int r2 = e / (nxv * 3);
+                const int r = r2 % ROWS;
+                const int b = r2 / ROWS;
+                const int kx = q / 3, c = q % 3;
+                S[(b * 3 * ROWS + r * 3 + c) * PL + kx] = stage[(b * ROWS + r) * RL + q];
+            }
+            __syncthreads();
+            constexpr int NP = NBIN * 3 * ROWS;
+            for (int e = tid; e < NP * (M / 2 + 1); e += ROW_THREADS) {
+                const int k = e % (M / 2 + 1);
+                const int p = e / (M / 2 + 1);
+                c2r_pre<T, N>(S + p * PL, tw, k);
+            }
+            __syncthreads();
+            dif<T, M, true, NP, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
+
+            if constexpr (MODE == RM_C2R || WRITE_RU) {
+                // real u (first 3*ROWS pencils) to rout, natural x order
+                for (int e = tid; e < ROWS * N * 3; e += ROW_THREADS) {
+                    const int c = e % 3;
+                    const int r2 = e / 3;
+                    const int x = r2 % N;
+                    const int r = r2 / N;
+                    const cpx<T> z = S[(r * 3 + c) * PL + dif_position<M>(x >> 1)];
+                    rout[((row0 + r) * N + x) * 3 + c] = (x & 1) ? z.y : z.x;
+                }
+            }
+            if constexpr (MODE == RM_C2R) {
+                __syncthreads();
+                continue;
+            }
+            if constexpr (WRITE_RU) __syncthreads();
+            if constexpr (MODE == RM_NONLIN) {
+                // u x w / npoints at each position (two grid points per position)
+                const T inv_np = (T)1 / ((T)N * (T)N * (T)N);
+                for (int e = tid; e < ROWS * M; e += ROW_THREADS) {
+                    const int p = e % M;
+                    const int r = e / M;
+                    cpx<T> u[3], w[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        u[c] = S[(r * 3 + c) * PL + p];
+                        w[c] = S[(3 * ROWS + r * 3 + c) * PL + p];
+                    }
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                        const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+                        const T tx = u[c1].x * w[c2].x - u[c2].x * w[c1].x;
+                        const T ty = u[c1].y * w[c2].y - u[c2].y * w[c1].y;
+                        S[(r * 3 + cc) * PL + p] = mk<T>(tx * inv_np, ty * inv_np);
+                    }
+                }
+                __syncthreads();
+            }
         }
+        // forward: digit-reversed -> natural, then R2C post-processing
+        dit<T, M, false, 3 * ROWS, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
+        for (int e = tid; e < 3 * ROWS * (M / 2 + 1); e += ROW_THREADS) {
+            const int k = e % (M / 2 + 1);
+            const int p = e / (M / 2 + 1);
+            r2c_post<T, N>(S + p * PL, tw, k);
+        }
+        __syncthreads();
+        for (int e = tid; e < ROWS * nxv * 3; e += ROW_THREADS) {
+            const int q = e % (nxv * 3);
+            const int r = e / (nxv * 3);
+            const int kx = q / 3, c = q % 3;
+            wout[(row0 + r) * nxp3 + q] = S[(r * 3 + c) * PL + kx];
+        }
+        __syncthreads();
     }
-    // forward: digit-reversed -> natural, then R2C post-processing
-    dit<T, M, false, 3 * ROWS, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
-    for (int e = tid; e < 3 * ROWS * (M / 2 + 1); e += ROW_THREADS) {
-        const int k = e % (M / 2 + 1);
-        const int p = e / (M / 2 + 1);
-        r2c_post<T, N>(S + p * PL, tw, k);
-    }
-    __syncthreads();
-    for (int e = tid; e < ROWS * nxv * 3; e += ROW_THREADS) {
-        const int q = e % (nxv * 3);
-        const int r = e / (nxv * 3);
-        const int kx = q / 3, c = q % 3;
-        wout[(row0 + r) * nxp3 + q] = S[(r * 3 + c) * PL + kx];
-    }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------

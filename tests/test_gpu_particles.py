@@ -62,3 +62,36 @@ def test_nsveparticles_steps_match_oracle(nm, nsteps):
     assert rel_err(ve.get_cvorticity(), ref.cvorticity) < 1e-10
     ps.close()
     ve.close()
+
+
+def test_arbitrary_global_indices_come_back_sorted():
+    # tracers given out of index order (as after an MPI redistribute) are
+    # written back in global index order (particles_output_hdf5.hpp)
+    from bfps_b200.solver import vorticity_equation, particles_system
+    n = 32
+    ve = vorticity_equation(n, precision="double")
+    w0 = ic.vorticity_ic(n, seed=2)
+    ve.set_cvorticity(w0)
+    ve.velocity_rspace()
+    ref = O.VorticityEquation(n)
+    ur = ref.ift(ref.compute_velocity(w0))
+    rng = np.random.default_rng(3)
+    pos = ic.tracer_ic(500, seed=9)
+    perm = rng.permutation(500)
+    gidx = 1000 + perm * 7  # any distinct global indices
+    ps = particles_system(ve, pos, 2, 1, nsteps=3, idx=gidx)
+    got = ps.sample_velocity()
+    want = P.sample(ur, pos, 2, 1, P.Geometry(n, n, n))
+    order = np.argsort(gidx)
+    assert rel_err(got, want[order]) < 1e-12
+    for _ in range(5):
+        ps.completeLoop(0.01)
+    p, r, idx = ps.state()
+    assert np.array_equal(idx, np.sort(gidx))
+    rps = P.ParticlesSystem(pos, np.zeros((3, 500, 3)), 2, 1, P.Geometry(n, n, n))
+    for _ in range(5):
+        rps.complete_loop(ur, 0.01)
+    assert rel_err(p, rps.pos[order]) < 1e-12
+    assert rel_err(r, rps.rhs[:, order]) < 1e-12
+    ps.close()
+    ve.close()
