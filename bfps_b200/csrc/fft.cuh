@@ -177,9 +177,14 @@ __device__ __forceinline__ cpx<T> twiddle(const cpx<T>* tw, int idx) {
 
 // ----------------------------------------------------------- stages --
 // One DIF stage S of a length-L transform over P pencils.
-// PFAST: consecutive threads take consecutive pencils (pencils adjacent in
-// shared memory); otherwise consecutive threads take consecutive elements.
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+// MAP (thread -> butterfly order): 1 = consecutive threads take consecutive
+// pencils; 0 = consecutive threads take consecutive elements; 2 = elements
+// while a stage's butterfly span is >= 32, pencils below (keeps the 32 lanes
+// of a warp on distinct banks for pencils laid out with an odd pitch).
+__host__ __device__ constexpr bool map_pencil_fast(int MAP, int span) {
+    return MAP == 1 || (MAP == 2 && span < 32);
+}
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
 __device__ __forceinline__ void dif_stage(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
     constexpr int R = plan_radix(L, S);
     constexpr int Ls = plan_block(L, S);
@@ -188,7 +193,7 @@ __device__ __forceinline__ void dif_stage(cpx<T>* s, const cpx<T>* tw, int tid, 
     constexpr int NW = P * NBLK * span;
     for (int w = tid; w < NW; w += nthr) {
         int p, b, j;
-        if (PFAST) {
+        if (map_pencil_fast(MAP, span)) {
             p = w % P;
             const int r = w / P;
             j = r % span;
@@ -214,7 +219,7 @@ __device__ __forceinline__ void dif_stage(cpx<T>* s, const cpx<T>* tw, int tid, 
 }
 
 // One DIT stage S (stages run from the last DIF stage back to stage 0).
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
 __device__ __forceinline__ void dit_stage(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
     constexpr int R = plan_radix(L, S);
     constexpr int Ls = plan_block(L, S);
@@ -223,7 +228,7 @@ __device__ __forceinline__ void dit_stage(cpx<T>* s, const cpx<T>* tw, int tid, 
     constexpr int NW = P * NBLK * span;
     for (int w = tid; w < NW; w += nthr) {
         int p, b, j;
-        if (PFAST) {
+        if (map_pencil_fast(MAP, span)) {
             p = w % P;
             const int r = w / P;
             j = r % span;
@@ -248,32 +253,32 @@ __device__ __forceinline__ void dit_stage(cpx<T>* s, const cpx<T>* tw, int tid, 
     }
 }
 
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
 __device__ __forceinline__ void dif_from(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
     if constexpr (S < plan_nstages(L)) {
-        dif_stage<T, L, S, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+        dif_stage<T, L, S, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
         __syncthreads();
-        dif_from<T, L, S + 1, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+        dif_from<T, L, S + 1, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
     }
 }
 // Full DIF transform: natural in, digit-reversed out.  Ends with a barrier.
-template <typename T, int L, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+template <typename T, int L, bool INV, int P, int PS, int ES, int MAP, int TAB>
 __device__ __forceinline__ void dif(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
-    dif_from<T, L, 0, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+    dif_from<T, L, 0, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
 }
 
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
 __device__ __forceinline__ void dit_down(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
     if constexpr (S >= 0) {
-        dit_stage<T, L, S, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+        dit_stage<T, L, S, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
         __syncthreads();
-        dit_down<T, L, S - 1, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+        dit_down<T, L, S - 1, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
     }
 }
 // Full DIT transform: digit-reversed in, natural out.  Ends with a barrier.
-template <typename T, int L, bool INV, int P, int PS, int ES, bool PFAST, int TAB>
+template <typename T, int L, bool INV, int P, int PS, int ES, int MAP, int TAB>
 __device__ __forceinline__ void dit(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
-    dit_down<T, L, plan_nstages(L) - 1, INV, P, PS, ES, PFAST, TAB>(s, tw, tid, nthr);
+    dit_down<T, L, plan_nstages(L) - 1, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
 }
 
 }  // namespace bfg

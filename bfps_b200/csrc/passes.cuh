@@ -246,7 +246,7 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
         }
 
         // ---- FFT along l: NB*W pencils, pencil stride 1, element stride PR --
-        dif<T, N, INV, NB * W, 1, PR, true, N>(tile, tw, tid, COL_THREADS);
+        dif<T, N, INV, NB * W, 1, PR, 1, N>(tile, tw, tid, COL_THREADS);
 
         // ---- epilogue ----------------------------------------------------
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
@@ -386,7 +386,7 @@ enum RowMode {
 constexpr int ROW_THREADS = 512;
 
 template <int N>
-__host__ __device__ constexpr int row_pl() { return N / 2 + 2; }
+__host__ __device__ constexpr int row_pl() { return N / 2 + 1; }  // odd pitch: pencils on distinct banks
 template <int N>
 __host__ __device__ constexpr int row_rl() { return (N / 2 + 4) * 3; }  // padded row, complex
 // staging (2 buffers) + pencils + twiddles for R rows
@@ -542,14 +542,15 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
             }
             __syncthreads();
         } else {
-            // transpose [r][kx][c] -> pencils [b][r][c][kx]
-            for (int e = tid; e < ROWS * NBIN * nxv * 3; e += ROW_THREADS) {
-                const int q = e % (nxv * 3);
-                const int r2 = e / (nxv * 3);
-                const int r = r2 % ROWS;
-                const int b = r2 / ROWS;
-                const int kx = q / 3, c = q % 3;
-                S[(b * 3 * ROWS + r * 3 + c) * PL + kx] = stage[(b * ROWS + r) * RL + q];
+            // transpose [r][kx][c] -> pencils [b][r][c][kx], kx fastest
+            // (staging read at stride 3, pencil write at stride 1)
+            for (int e = tid; e < ROWS * NBIN * 3 * nxv; e += ROW_THREADS) {
+                const int kx = e % nxv;
+                const int p = e / nxv;  // = b*3*ROWS + r*3 + c
+                const int c = p % 3;
+                const int r = (p / 3) % ROWS;
+                const int b = p / (3 * ROWS);
+                S[p * PL + kx] = stage[(b * ROWS + r) * RL + kx * 3 + c];
             }
             __syncthreads();
             constexpr int NP = NBIN * 3 * ROWS;
@@ -559,7 +560,7 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
                 c2r_pre<T, N>(S + p * PL, tw, k);
             }
             __syncthreads();
-            dif<T, M, true, NP, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
+            dif<T, M, true, NP, PL, 1, 2, N>(S, tw, tid, ROW_THREADS);
 
             if constexpr (MODE == RM_C2R || WRITE_RU) {
                 // real u (first 3*ROWS pencils) to rout, natural x order
@@ -601,7 +602,7 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
             }
         }
         // forward: digit-reversed -> natural, then R2C post-processing
-        dit<T, M, false, 3 * ROWS, PL, 1, false, N>(S, tw, tid, ROW_THREADS);
+        dit<T, M, false, 3 * ROWS, PL, 1, 2, N>(S, tw, tid, ROW_THREADS);
         for (int e = tid; e < 3 * ROWS * (M / 2 + 1); e += ROW_THREADS) {
             const int k = e % (M / 2 + 1);
             const int p = e / (M / 2 + 1);
