@@ -63,6 +63,7 @@ SIGNATURES = {
     "bfg_particles_info": (_i, [_vp, _c.POINTER(_i64), _c.POINTER(_i), _c.POINTER(_i)]),
     "bfg_last_step_ms": (_i, [_vp, _pd]),
     "bfg_kernel_launches": (_i, [_vp, _c.POINTER(_i64)]),
+    "bfg_rspace_stats_noalloc": (_i, [_vp, _i, _i, _i, _i, _d, _i, _vp, _vp, _vp]),
 }
 
 _LIB = None

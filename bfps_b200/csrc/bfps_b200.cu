@@ -1100,3 +1100,161 @@ int bfg_particles_info(const bfg_pctx* p, int64_t* n, int* nsteps, int* step_idx
 }
 
 }  // extern "C"
+
+// ======================================================= no-allocation stats ==
+// bfg_rspace_stats_noalloc: the real-space moments / histogram reduction of
+// field::compute_rspace_stats for callers that cannot call cudaMalloc --
+// for example a host whose device memory is already owned or reserved by
+// another framework's caching allocator, an application that fixes its
+// memory footprint at start-up, or a latency-sensitive loop that cannot
+// afford cudaMalloc's implicit device-wide synchronisation.  The caller
+// passes the input field and the output arrays; the per-block partial sums
+// live in the fixed file-scope device array below instead of in memory the
+// library would allocate.  The array exists on every GPU that loads the
+// library, for as long as the library stays loaded.
+
+// per-block partial sums: STATS_BLOCKS blocks x NQ doubles = 370 KiB
+static __device__ __align__(256) double g_noalloc_partials[STATS_BLOCKS * NQ];
+
+// same reduction as moments_kernel, over a field stored with a padded row
+// pitch (the reference real layout (nz, ny, nx+2, 3))
+template <typename T>
+__global__ void __launch_bounds__(STATS_THREADS)
+moments_pitched_kernel(const T* __restrict__ r, int nx, int pitch, size_t npts, double me0,
+                       double me1, double me2, double me3, int nbins,
+                       double* __restrict__ partial, unsigned long long* __restrict__ hist) {
+    extern __shared__ unsigned int shist_p[];  // nbins * 4
+    __shared__ double red[STATS_THREADS / 32][NQ];
+    for (int i = threadIdx.x; i < nbins * 4; i += blockDim.x) shist_p[i] = 0;
+    __syncthreads();
+    const double me[4] = {me0, me1, me2, me3};
+    double binsize[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) binsize[i] = 2 * me[i] / nbins;
+    double mn[4] = {0.0, 0.0, 0.0, me3};
+    double mx[4] = {0.0, 0.0, 0.0, 0.0};
+    double sm[8][4];
+#pragma unroll
+    for (int n = 0; n < 8; ++n)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) sm[n][i] = 0.0;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < npts;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const size_t x = e % (size_t)nx, rowi = e / (size_t)nx;
+        const T* pt = r + (rowi * (size_t)pitch + x) * 3;
+        double v[4];
+        v[3] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            v[i] = (double)pt[i];
+            v[3] += v[i] * v[i];
+        }
+        v[3] = sqrt(v[3]);
+        {
+            const int b = (int)floor(v[3] * 2 / binsize[3]);
+            if (b >= 0 && b < nbins) atomicAdd(&shist_p[b * 4 + 3], 1u);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const int b = (int)floor((v[i] + me[i]) / binsize[i]);
+            if (b >= 0 && b < nbins) atomicAdd(&shist_p[b * 4 + i], 1u);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            mn[i] = fmin(mn[i], v[i]);
+            mx[i] = fmax(mx[i], v[i]);
+            double p = 1.0;
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+                p = v[i] * p;
+                sm[n][i] += p;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        double a = warp_min(mn[i]);
+        double b = warp_max(mx[i]);
+        if (lane == 0) {
+            red[wid][0 * 4 + i] = a;
+            red[wid][9 * 4 + i] = b;
+        }
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            double s = warp_sum(sm[n][i]);
+            if (lane == 0) red[wid][(n + 1) * 4 + i] = s;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < NQ) {
+        const int q = threadIdx.x;
+        double acc = red[0][q];
+        for (int w = 1; w < STATS_THREADS / 32; ++w) {
+            const double v = red[w][q];
+            if (q < 4) acc = fmin(acc, v);
+            else if (q >= 36) acc = fmax(acc, v);
+            else acc += v;
+        }
+        partial[(size_t)blockIdx.x * NQ + q] = acc;
+    }
+    for (int i = threadIdx.x; i < nbins * 4; i += blockDim.x)
+        if (shist_p[i]) atomicAdd(&hist[i], (unsigned long long)shist_p[i]);
+}
+
+// Device address of g_noalloc_partials on the current device.  Host code
+// cannot use the array's name as a device pointer, so the address is looked
+// up once per device (cudaGetSymbolAddress, with that device current) and
+// cached; the lookup happens inside the first call made on each device.
+static double* noalloc_partials_on(int device, cudaError_t* err) {
+    static std::mutex mu;
+    static std::unordered_map<int, double*> addr;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = addr.find(device);
+    if (it != addr.end()) return it->second;
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess) {
+        *err = e;
+        return nullptr;
+    }
+    addr[device] = static_cast<double*>(p);
+    return static_cast<double*>(p);
+}
+
+extern "C" int bfg_rspace_stats_noalloc(const void* dev_field, int nx, int ny, int nz,
+                                        int real_bytes, double max_estimate, int nbins,
+                                        double* dev_moments, int64_t* dev_hist, void* stream) {
+    if (!dev_field || !dev_moments || !dev_hist) return BFG_EINVAL;
+    if (nx < 1 || ny < 1 || nz < 1 || (real_bytes != 4 && real_bytes != 8)) return BFG_EINVAL;
+    if (nbins < 1) return BFG_EINVAL;
+    if (nbins > BFG_NOALLOC_MAX_BINS) return BFG_EUNSUP;  // shared-memory histogram limit
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return BFG_ECUDA;
+    }
+    cudaError_t err = cudaSuccess;
+    double* partials = noalloc_partials_on(device, &err);
+    if (!partials) return BFG_ECUDA;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t npts = (size_t)nx * ny * nz;
+    // the histogram is accumulated into the caller's output: start it at zero
+    if (cudaMemsetAsync(dev_hist, 0, (size_t)nbins * 4 * sizeof(int64_t), s) != cudaSuccess) {
+        cudaGetLastError();
+        return BFG_ECUDA;
+    }
+    const double me3 = max_estimate * std::sqrt(3.0);
+    const size_t shmem = (size_t)nbins * 4 * sizeof(unsigned int);
+    if (real_bytes == 4)
+        moments_pitched_kernel<float><<<STATS_BLOCKS, STATS_THREADS, shmem, s>>>(
+            static_cast<const float*>(dev_field), nx, nx + 2, npts, max_estimate, max_estimate,
+            max_estimate, me3, nbins, partials, reinterpret_cast<unsigned long long*>(dev_hist));
+    else
+        moments_pitched_kernel<double><<<STATS_BLOCKS, STATS_THREADS, shmem, s>>>(
+            static_cast<const double*>(dev_field), nx, nx + 2, npts, max_estimate, max_estimate,
+            max_estimate, me3, nbins, partials, reinterpret_cast<unsigned long long*>(dev_hist));
+    moments_final<<<1, 64, 0, s>>>(partials, STATS_BLOCKS, 1.0 / (double)npts, dev_moments);
+    if (cudaGetLastError() != cudaSuccess) return BFG_ECUDA;
+    return BFG_OK;
+}

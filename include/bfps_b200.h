@@ -181,6 +181,34 @@ int bfg_profile_read(bfg_ctx* ctx, int kind, double* total_ms, int64_t* launches
 /* Count of kernels the library launched since the context was created. */
 int bfg_kernel_launches(const bfg_ctx* ctx, int64_t* count);
 
+/* ------------------------------------------------- no-allocation stats ---- */
+
+/* No counterpart in the reference: an extra entry point for callers that
+ * cannot call cudaMalloc (device memory already owned or reserved by another
+ * framework's allocator, a footprint fixed at start-up, or a loop that
+ * cannot afford cudaMalloc's device-wide synchronisation).
+ *
+ * Computes the real-space moments (10, 4) f64 and histogram (nbins, 4) i64 of
+ * field::compute_rspace_stats (field.cpp:661-889) for a real 3-vector field
+ * in the reference layout (nz, ny, nx+2, 3) (float if real_bytes == 4, else
+ * double).  max_estimate is the per-component estimate (the magnitude uses
+ * max_estimate * sqrt(3)).  All pointers are device pointers supplied by the
+ * caller; the work is queued on `stream` (NULL: the default stream) and the
+ * call returns without waiting for it.
+ *
+ * Allocates nothing: the per-block partial sums live in a fixed 370 KiB
+ * device array inside the library, present on every GPU that loads it until
+ * the library is unloaded.  The first call on a device looks up that
+ * array's device address (with the device current) and should come before
+ * any stream capture.  All calls share the array, so calls that overlap on
+ * the GPU (for example on two streams at once) race; order them.  The
+ * histogram output is cleared by the call itself.  nbins above
+ * BFG_NOALLOC_MAX_BINS returns BFG_EUNSUP. */
+#define BFG_NOALLOC_MAX_BINS 2048
+int bfg_rspace_stats_noalloc(const void* dev_field, int nx, int ny, int nz, int real_bytes,
+                             double max_estimate, int nbins, double* dev_moments,
+                             int64_t* dev_hist, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
