@@ -176,35 +176,56 @@ __device__ __forceinline__ cpx<T> twiddle(const cpx<T>* tw, int idx) {
 }
 
 // ----------------------------------------------------------- stages --
-// One DIF stage S of a length-L transform over P pencils.
+// Pencil layout in shared memory: pencil p starts at
+//   base(p) = (p / PG) * GS + (p % PG) * PS
+// and its element e sits at base(p) + e * ES.  Examples: pencils side by side
+// in a tile row (PG = 1, GS = 1, ES = row pitch); contiguous pencils
+// (PG = 1, GS = pitch, ES = 1); the three components of interleaved rows
+// (PG = 3, GS = row length, PS = 1, ES = 3).
+template <int PG_, int GS_, int PS_, int ES_>
+struct Lay {
+    static constexpr int PG = PG_, GS = GS_, PS = PS_, ES = ES_;
+    __device__ __forceinline__ static int base(int p) {
+        return PG == 1 ? p * GS : (p / PG) * GS + (p % PG) * PS;
+    }
+};
+
 // MAP (thread -> butterfly order): 1 = consecutive threads take consecutive
 // pencils; 0 = consecutive threads take consecutive elements; 2 = elements
-// while a stage's butterfly span is >= 32, pencils below (keeps the 32 lanes
-// of a warp on distinct banks for pencils laid out with an odd pitch).
+// while a stage's butterfly span is >= 32, pencils below.
 __host__ __device__ constexpr bool map_pencil_fast(int MAP, int span) {
     return MAP == 1 || (MAP == 2 && span < 32);
 }
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
+
+// decode work item w of stage (P pencils, NBLK blocks, span) into (p, b, j)
+template <int P, int NBLK, int span, bool PF>
+__device__ __forceinline__ void stage_item(int w, int& p, int& b, int& j) {
+    if (PF) {
+        p = w % P;
+        const int r = w / P;
+        j = r % span;
+        b = r / span;
+    } else {
+        j = w % span;
+        const int r = w / span;
+        b = r % NBLK;
+        p = r / NBLK;
+    }
+}
+
+// One DIF stage S of a length-L transform over P pencils.
+template <typename T, int L, int S, bool INV, int P, class LAY, int MAP, int TAB>
 __device__ __forceinline__ void dif_stage(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
     constexpr int R = plan_radix(L, S);
     constexpr int Ls = plan_block(L, S);
     constexpr int span = Ls / R;
     constexpr int NBLK = L / Ls;
     constexpr int NW = P * NBLK * span;
+    constexpr int ES = LAY::ES;
     for (int w = tid; w < NW; w += nthr) {
         int p, b, j;
-        if (map_pencil_fast(MAP, span)) {
-            p = w % P;
-            const int r = w / P;
-            j = r % span;
-            b = r / span;
-        } else {
-            j = w % span;
-            const int r = w / span;
-            b = r % NBLK;
-            p = r / NBLK;
-        }
-        const int base = p * PS + (b * Ls + j) * ES;
+        stage_item<P, NBLK, span, map_pencil_fast(MAP, span)>(w, p, b, j);
+        const int base = LAY::base(p) + (b * Ls + j) * ES;
         cpx<T> v[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) v[m] = s[base + m * span * ES];
@@ -219,27 +240,18 @@ __device__ __forceinline__ void dif_stage(cpx<T>* s, const cpx<T>* tw, int tid, 
 }
 
 // One DIT stage S (stages run from the last DIF stage back to stage 0).
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
+template <typename T, int L, int S, bool INV, int P, class LAY, int MAP, int TAB>
 __device__ __forceinline__ void dit_stage(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
     constexpr int R = plan_radix(L, S);
     constexpr int Ls = plan_block(L, S);
     constexpr int span = Ls / R;
     constexpr int NBLK = L / Ls;
     constexpr int NW = P * NBLK * span;
+    constexpr int ES = LAY::ES;
     for (int w = tid; w < NW; w += nthr) {
         int p, b, j;
-        if (map_pencil_fast(MAP, span)) {
-            p = w % P;
-            const int r = w / P;
-            j = r % span;
-            b = r / span;
-        } else {
-            j = w % span;
-            const int r = w / span;
-            b = r % NBLK;
-            p = r / NBLK;
-        }
-        const int base = p * PS + (b * Ls + j) * ES;
+        stage_item<P, NBLK, span, map_pencil_fast(MAP, span)>(w, p, b, j);
+        const int base = LAY::base(p) + (b * Ls + j) * ES;
         cpx<T> v[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) v[m] = s[base + m * span * ES];
@@ -253,32 +265,49 @@ __device__ __forceinline__ void dit_stage(cpx<T>* s, const cpx<T>* tw, int tid, 
     }
 }
 
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
-__device__ __forceinline__ void dif_from(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
-    if constexpr (S < plan_nstages(L)) {
-        dif_stage<T, L, S, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
+// DIF stages [S, SEND), each followed by a barrier.
+template <typename T, int L, int S, int SEND, bool INV, int P, class LAY, int MAP, int TAB>
+__device__ __forceinline__ void dif_range(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    if constexpr (S < SEND) {
+        dif_stage<T, L, S, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
         __syncthreads();
-        dif_from<T, L, S + 1, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
+        dif_range<T, L, S + 1, SEND, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
     }
 }
 // Full DIF transform: natural in, digit-reversed out.  Ends with a barrier.
-template <typename T, int L, bool INV, int P, int PS, int ES, int MAP, int TAB>
+template <typename T, int L, bool INV, int P, class LAY, int MAP, int TAB>
 __device__ __forceinline__ void dif(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
-    dif_from<T, L, 0, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
+    dif_range<T, L, 0, plan_nstages(L), INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
 }
 
-template <typename T, int L, int S, bool INV, int P, int PS, int ES, int MAP, int TAB>
+template <typename T, int L, int S, bool INV, int P, class LAY, int MAP, int TAB>
 __device__ __forceinline__ void dit_down(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
     if constexpr (S >= 0) {
-        dit_stage<T, L, S, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
+        dit_stage<T, L, S, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
         __syncthreads();
-        dit_down<T, L, S - 1, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
+        dit_down<T, L, S - 1, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
     }
 }
 // Full DIT transform: digit-reversed in, natural out.  Ends with a barrier.
-template <typename T, int L, bool INV, int P, int PS, int ES, int MAP, int TAB>
+template <typename T, int L, bool INV, int P, class LAY, int MAP, int TAB>
 __device__ __forceinline__ void dit(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
-    dit_down<T, L, plan_nstages(L) - 1, INV, P, PS, ES, MAP, TAB>(s, tw, tid, nthr);
+    dit_down<T, L, plan_nstages(L) - 1, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
+}
+
+// frequency held at DIF output position p of a length-L transform
+template <int L>
+__device__ __forceinline__ int dif_frequency(int p) {
+    int k = 0, mult = 1, Lr = L, rem = p;
+#pragma unroll
+    for (int s = 0; s < plan_nstages(L); ++s) {
+        const int R = plan_step(Lr);
+        Lr /= R;
+        const int q = rem / Lr;
+        rem -= q * Lr;
+        k += q * mult;
+        mult *= R;
+    }
+    return k;
 }
 
 }  // namespace bfg

@@ -121,6 +121,10 @@ __device__ __forceinline__ void divfree(A kx, A ky, A kz, A inv_k2, cpx<A>* a) {
 template <typename T>
 __device__ __forceinline__ cpx<T> zero_c() { return mk<T>((T)0, (T)0); }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // global row of tile row l (input side) / lo (output side) for a pass mode
 template <int N, int MODE>
 __device__ __forceinline__ size_t col_in_row(int a, int l) {
@@ -143,6 +147,97 @@ __device__ __forceinline__ size_t col_out_row(int a, int lo) {
 //      [f][0..NXV) kx, [f][NXV..NXV+N) ky, [f][NXV+N..NXV+2N) kz, where
 //      f = 0: exp(-nu k^2 dt), 1: exp(-nu k^2 dt/2), 2: exp(+nu k^2 dt/2)
 //      per axis (their product over the axes is the factor of k^2).
+// FZ epilogue for one mode (l = kz, ix): dealias, i k x, forcing,
+// force_divfree, RK update of stage MODE (vorticity_equation.cpp:290-437)
+template <typename T, int N, int MODE>
+__device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, int PR, int a, int l,
+                                         int ix, int col, double ky, const cpx<T>* v0,
+                                         const cpx<T>* vp, size_t pt, const T* __restrict__ filt,
+                                         const T* __restrict__ fac, const cpx<T>* __restrict__ fsrc,
+                                         cpx<T>* out0) {
+    const int nxv = kp.nxv;
+    const double kz = kwrap<N>(l, kp.dkz);
+    const double kx = (double)ix * kp.dkx;
+    const double k2 = (kx * kx + ky * ky) + kz * kz;
+    const int p = dif_position<N>(l);
+    cpx<T> nl[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) nl[c] = tile[p * PR + col * 3 + c];
+    // dealias (kspace.cpp:461-485)
+    if (kp.dealias == 1) {
+        int key = (int)rint(k2 * kp.inv_dk2);
+        key = key < kp.nfilt ? key : kp.nfilt - 1;
+        const T f = filt[key];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nl[c] = scale(nl[c], f);
+    } else if (k2 >= kp.kM2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nl[c] = zero_c<T>();
+    }
+    // i k x (vorticity_equation.cpp:323-350)
+    cpx<T> tt[3];
+    curl<T>((T)kx, (T)ky, (T)kz, nl, tt);
+    // forcing (vorticity_equation.cpp:241-288), factor 1
+    if (kp.forcing == 1) {
+        const double kn = sqrt(k2);
+        if (kp.fk0 <= kn && kp.fk1 >= kn) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const cpx<T> fv = fsrc[pt * 3 + c];
+                tt[c].x += (T)(kp.famp * (double)fv.x);
+                tt[c].y += (T)(kp.famp * (double)fv.y);
+            }
+        }
+    } else if (kp.forcing == 2) {
+        if (ix == 0 && l == 0) {
+            if (a == kp.fmode) tt[2].x -= (T)(kp.famp / 2);
+            if (a == N - kp.fmode) tt[2].x -= (T)(kp.famp / 2);
+        }
+    }
+    // force_divfree on the nonlinear term; zero mode cleared
+    const bool kzero = (a == 0 && l == 0 && ix == 0);
+    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), tt);
+    if (kzero) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tt[c] = zero_c<T>();
+    }
+    // RK update (vorticity_equation.cpp:366-434), only for k2 <= kM2
+    const bool inside = k2 <= kp.kM2;
+    const T dt = (T)kp.dt;
+    cpx<T> o[3];
+    const int nfac = nxv + 2 * N;
+    if (MODE == CM_FZ_RK1) {
+        const T f0 = fac[ix] * fac[nxv + a] * fac[nxv + N + l];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            o[c] = inside ? mk<T>((v0[c].x + dt * tt[c].x) * f0, (v0[c].y + dt * tt[c].y) * f0)
+                          : zero_c<T>();
+    } else if (MODE == CM_FZ_RK2) {
+        const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
+        const T f1 = fac[2 * nfac + ix] * fac[2 * nfac + nxv + a] * fac[2 * nfac + nxv + N + l];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            o[c] = inside ? mk<T>((3 * v0[c].x * f0 + (vp[c].x + dt * tt[c].x) * f1) * (T)0.25,
+                                  (3 * v0[c].y * f0 + (vp[c].y + dt * tt[c].y) * f1) * (T)0.25)
+                          : zero_c<T>();
+    } else {
+        const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            o[c] = inside ? mk<T>((v0[c].x * f0 + 2 * (vp[c].x + dt * tt[c].x)) * f0 / (T)3,
+                                  (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 / (T)3)
+                          : v0[c];
+        // final force_divfree of the state (vorticity_equation.cpp:436)
+        if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), o);
+        if (kzero) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out0[pt * 3 + c] = o[c];
+}
+
 template <typename T, int N, int MODE>
 __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
                                                const cpx<T>* in1, int a, int kx0, int ncol,
@@ -208,6 +303,25 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
                 const int kx0n = (tn % ntx) * TKX;
                 col_issue_load<T, N, MODE>(bufs + ((it + 1) & 1) * TILE, in0, in1, tn / ntx, kx0n,
                                            min(TKX, kp.nxv - kx0n), nxp3, tid);
+                if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
+                    // RK operands of the next tile into L2 while this tile is transformed
+                    constexpr int LINES = (W * (int)sizeof(cpx<T>) + 127) / 128 + 1;
+                    constexpr int NARR = (MODE == CM_FZ_RK1) ? 1 : 2;
+                    const int an = tn / ntx;
+                    for (int e = tid; e < N * NARR * LINES; e += COL_THREADS) {
+                        const int ln = e % LINES;
+                        const int r = e / LINES;
+                        const int arr = r % NARR;
+                        const int l = r / NARR;
+                        const char* base = reinterpret_cast<const char*>(
+                            ((arr == 0) ? rk_v0 : rk_vp) + ((size_t)an * N + l) * nxp3 +
+                            (size_t)kx0n * 3);
+                        const char* a0 = reinterpret_cast<const char*>(
+                            reinterpret_cast<uintptr_t>(base) & ~(uintptr_t)127);
+                        const char* pl = a0 + ln * 128;
+                        if (pl < base + W * (int)sizeof(cpx<T>)) prefetch_l2(pl);
+                    }
+                }
             }
             cp_async_commit();
         }
@@ -246,130 +360,66 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
         }
 
         // ---- FFT along l: NB*W pencils, pencil stride 1, element stride PR --
-        dif<T, N, INV, NB * W, 1, PR, 1, N>(tile, tw, tid, COL_THREADS);
-
-        // ---- epilogue ----------------------------------------------------
+        using LY = Lay<1, 1, 0, PR>;
+        constexpr int P = NB * W;
+        constexpr int NST = plan_nstages(N);
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
+            dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, COL_THREADS);
+            // ---- epilogue: per point, two points per batch so that the RK
+            // operand loads of both are in flight together
             const double ky = kwrap<N>(a, kp.dky);
-            const int nxv = kp.nxv;
-            for (int e = tid; e < N * TKX; e += COL_THREADS) {
-                const int col = e % TKX;
-                const int l = e / TKX;  // output kz index
-                if (col >= ncol) continue;
-                const int ix = kx0 + col;
-                const size_t pt = ((size_t)a * N + l) * kp.nxp + ix;  // S[ky=a][kz=l][kx]
-                // RK operands first, so their latency overlaps the k-space math
-                cpx<T> v0[3], vp[3];
+            for (int e0 = tid; e0 < N * TKX; e0 += 2 * COL_THREADS) {
+                cpx<T> v0[2][3], vp[2][3];
+                size_t pt[2];
+                bool ok[2];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) v0[c] = rk_v0[pt * 3 + c];
-                if (MODE != CM_FZ_RK1) {
+                for (int h = 0; h < 2; ++h) {
+                    const int e = e0 + h * COL_THREADS;
+                    const int col = e % TKX;
+                    const int l = e / TKX;
+                    ok[h] = e < N * TKX && col < ncol;
+                    pt[h] = ((size_t)a * N + l) * kp.nxp + kx0 + col;  // S[ky=a][kz=l][kx]
+                    if (ok[h]) {
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) vp[c] = rk_vp[pt * 3 + c];
-                }
-                const double kz = kwrap<N>(l, kp.dkz);
-                const double kx = (double)ix * kp.dkx;
-                const double k2 = (kx * kx + ky * ky) + kz * kz;
-                const int p = dif_position<N>(l);
-                cpx<T> nl[3];
+                        for (int c = 0; c < 3; ++c) v0[h][c] = rk_v0[pt[h] * 3 + c];
+                        if (MODE != CM_FZ_RK1) {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) nl[c] = tile[p * PR + col * 3 + c];
-                // dealias (kspace.cpp:461-485)
-                if (kp.dealias == 1) {
-                    int key = (int)rint(k2 * kp.inv_dk2);
-                    key = key < kp.nfilt ? key : kp.nfilt - 1;
-                    const T f = filt[key];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) nl[c] = scale(nl[c], f);
-                } else if (k2 >= kp.kM2) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) nl[c] = zero_c<T>();
-                }
-                // i k x (vorticity_equation.cpp:323-350)
-                cpx<T> tt[3];
-                curl<T>((T)kx, (T)ky, (T)kz, nl, tt);
-                // forcing (vorticity_equation.cpp:241-288), factor 1
-                if (kp.forcing == 1) {
-                    const double kn = sqrt(k2);
-                    if (kp.fk0 <= kn && kp.fk1 >= kn) {
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            const cpx<T> fv = fsrc[pt * 3 + c];
-                            tt[c].x += (T)(kp.famp * (double)fv.x);
-                            tt[c].y += (T)(kp.famp * (double)fv.y);
+                            for (int c = 0; c < 3; ++c) vp[h][c] = rk_vp[pt[h] * 3 + c];
                         }
                     }
-                } else if (kp.forcing == 2) {
-                    if (ix == 0 && l == 0) {
-                        if (a == kp.fmode) tt[2].x -= (T)(kp.famp / 2);
-                        if (a == N - kp.fmode) tt[2].x -= (T)(kp.famp / 2);
-                    }
-                }
-                // force_divfree on the nonlinear term; zero mode cleared
-                const bool kzero = (a == 0 && l == 0 && ix == 0);
-                if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), tt);
-                if (kzero) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) tt[c] = zero_c<T>();
-                }
-                // RK update (vorticity_equation.cpp:366-434), only for k2 <= kM2
-                const bool inside = k2 <= kp.kM2;
-                const T dt = (T)kp.dt;
-                cpx<T> o[3];
-                const int nfac = nxv + 2 * N;
-                if (MODE == CM_FZ_RK1) {
-                    const T f0 = fac[ix] * fac[nxv + a] * fac[nxv + N + l];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-                        o[c] = inside ? mk<T>((v0[c].x + dt * tt[c].x) * f0,
-                                              (v0[c].y + dt * tt[c].y) * f0)
-                                      : zero_c<T>();
-                } else if (MODE == CM_FZ_RK2) {
-                    const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
-                    const T f1 = fac[2 * nfac + ix] * fac[2 * nfac + nxv + a] *
-                                 fac[2 * nfac + nxv + N + l];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-                        o[c] = inside
-                                   ? mk<T>((3 * v0[c].x * f0 + (vp[c].x + dt * tt[c].x) * f1) * (T)0.25,
-                                           (3 * v0[c].y * f0 + (vp[c].y + dt * tt[c].y) * f1) * (T)0.25)
-                                   : zero_c<T>();
-                } else {
-                    const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-                        o[c] = inside ? mk<T>((v0[c].x * f0 + 2 * (vp[c].x + dt * tt[c].x)) * f0 / (T)3,
-                                              (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 / (T)3)
-                                      : v0[c];
-                    // final force_divfree of the state (vorticity_equation.cpp:436)
-                    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), o);
-                    if (kzero) {
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
-                    }
                 }
 #pragma unroll
-                for (int c = 0; c < 3; ++c) out0[pt * 3 + c] = o[c];
+                for (int h = 0; h < 2; ++h) {
+                    if (!ok[h]) continue;
+                    const int e = e0 + h * COL_THREADS;
+                    const int col = e % TKX;
+                    const int l = e / TKX;  // output kz index
+                    fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, ky, v0[h], vp[h],
+                                         pt[h], filt, fac, fsrc, out0);
+                }
             }
         } else {
-            // plain store of NB buffers, output row lo (natural order); whole
-            // vectors inside the valid columns, single complex at the edge
+            dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, COL_THREADS);
+            // last stage fused with the store: block b of R positions holds
+            // frequencies f(b) + (N/R) q; lanes take consecutive pencils, i.e.
+            // consecutive complex numbers of one output row chunk
+            constexpr int R = plan_radix(N, NST - 1);
+            constexpr int NW = P * (N / R);
             const int nval = 3 * ncol;
-            for (int e = tid; e < N * NB * WV; e += COL_THREADS) {
-                const int v = e % WV;
-                const int r = e / WV;
-                const int b = r % NB;
-                const int lo = r / NB;
-                const int q = v * VPE;
+            for (int w = tid; w < NW; w += COL_THREADS) {
+                const int pp = w % P;
+                const int bb = w / P;
+                cpx<T> v[R];
+#pragma unroll
+                for (int m = 0; m < R; ++m) v[m] = tile[pp + (bb * R + m) * PR];
+                dft<T, INV, R>(v);
+                const int bufi = pp / W, q = pp % W;
                 if (q >= nval) continue;
-                const size_t row = col_out_row<N, MODE>(a, lo);
-                const int p = dif_position<N>(lo);
-                cpx<T>* dst = ((b == 0) ? out0 : out1) + row * nxp3 + (size_t)kx0 * 3 + q;
-                const cpx<T>* sp = &tile[p * PR + b * W + q];
-                if (q + VPE <= nval) {
-                    *reinterpret_cast<V*>(dst) = *reinterpret_cast<const V*>(sp);
-                } else {
-                    for (int u = 0; u < nval - q; ++u) dst[u] = sp[u];
-                }
+                cpx<T>* dst = ((bufi == 0) ? out0 : out1) + (size_t)kx0 * 3 + q;
+                const int f0 = dif_frequency<N>(bb * R);
+#pragma unroll
+                for (int m = 0; m < R; ++m)
+                    dst[col_out_row<N, MODE>(a, f0 + (N / R) * m) * nxp3] = v[m];
             }
         }
         __syncthreads();  // this buffer is refilled by the load issued next iteration
@@ -386,16 +436,15 @@ enum RowMode {
 constexpr int ROW_THREADS = 512;
 
 template <int N>
-__host__ __device__ constexpr int row_pl() { return N / 2 + 1; }  // odd pitch: pencils on distinct banks
-template <int N>
 __host__ __device__ constexpr int row_rl() { return (N / 2 + 4) * 3; }  // padded row, complex
-// staging (2 buffers) + pencils + twiddles for R rows
+// shared memory for R rows: staging (two alternating buffers; the FFTs run in
+// place on the interleaved [kx][c] rows), twiddles, digit-reversal table
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t row_bytes_for(int R) {
-    return (size_t)((MODE == RM_R2C) ? 2 * R * (N * 3 / 2)             // real rows, as complex pairs
-                                     : 2 * R * (MODE == RM_NONLIN ? 2 : 1) * row_rl<N>()) *
-               sizeof(cpx<T>) +
-           (size_t)((MODE == RM_NONLIN ? 6 : 3) * R * row_pl<N>() + N) * sizeof(cpx<T>);
+    return (MODE == RM_R2C)
+               ? (size_t)(2 * R * (N * 3 / 2) + R * row_rl<N>() + N) * sizeof(cpx<T>) + (N / 2) * 4
+               : (size_t)(2 * R * (MODE == RM_NONLIN ? 2 : 1) * row_rl<N>() + N) * sizeof(cpx<T>) +
+                     (N / 2) * 4;
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int row_rows_from(int R) {
@@ -412,67 +461,69 @@ __host__ __device__ constexpr size_t row_smem_bytes() {
     return row_bytes_for<T, N, MODE>(row_rows<T, N, MODE>());
 }
 
-// C2R pre-processing of one pencil (k, M-k pairs), X[0], X[M] real parts.
-template <typename T, int N>
+// C2R pre-processing of one pencil (element stride ES): pairs (k, M-k),
+// X[0] and X[M] enter with their real parts only.
+template <typename T, int N, int ES>
 __device__ __forceinline__ void c2r_pre(cpx<T>* s, const cpx<T>* tw, int k) {
     constexpr int M = N / 2;
     if (k == 0) {
-        const T x0 = s[0].x, xm = s[M].x;
+        const T x0 = s[0].x, xm = s[M * ES].x;
         s[0] = mk<T>(x0 + xm, x0 - xm);
         return;
     }
-    const cpx<T> a = s[k], b = s[M - k];
+    const cpx<T> a = s[k * ES], b = s[(M - k) * ES];
     const cpx<T> w = tw[k];  // exp(-2 pi i k / N)
     // Z[k] = (a + conj b) + i conj(w) (a - conj b)
     {
         const cpx<T> sp = a + conjg(b), dm = a - conjg(b);
         const cpx<T> e = cmulc(dm, w);  // dm * conj(w)
-        s[k] = mk<T>(sp.x - e.y, sp.y + e.x);
+        s[k * ES] = mk<T>(sp.x - e.y, sp.y + e.x);
     }
     if (k != M - k) {
         // Z[M-k] = (b + conj a) - i w (b - conj a)
         const cpx<T> sp = b + conjg(a), dm = b - conjg(a);
         const cpx<T> e = cmul(dm, w);
-        s[M - k] = mk<T>(sp.x + e.y, sp.y - e.x);
+        s[(M - k) * ES] = mk<T>(sp.x + e.y, sp.y - e.x);
     }
 }
 
 // R2C post-processing of one pencil (natural-order Z), writes X[0..M].
-template <typename T, int N>
+template <typename T, int N, int ES>
 __device__ __forceinline__ void r2c_post(cpx<T>* s, const cpx<T>* tw, int k) {
     constexpr int M = N / 2;
     const T h = (T)0.5;
     if (k == 0) {
         const cpx<T> z0 = s[0];
         s[0] = mk<T>(z0.x + z0.y, (T)0);
-        s[M] = mk<T>(z0.x - z0.y, (T)0);
+        s[M * ES] = mk<T>(z0.x - z0.y, (T)0);
         return;
     }
-    const cpx<T> zk = s[k], zm = s[M - k];
+    const cpx<T> zk = s[k * ES], zm = s[(M - k) * ES];
     const cpx<T> w = tw[k];
     {
         const cpx<T> e = scale(zk + conjg(zm), h);
         const cpx<T> d = zk - conjg(zm);
         const cpx<T> o = mk<T>(d.y * h, -d.x * h);  // d / (2i)
-        s[k] = e + cmul(w, o);
+        s[k * ES] = e + cmul(w, o);
     }
     if (k != M - k) {
         // exp(-2 pi i (M-k)/N) = -conj(w)
         const cpx<T> e = scale(zm + conjg(zk), h);
         const cpx<T> d = zm - conjg(zk);
         const cpx<T> o = mk<T>(d.y * h, -d.x * h);
-        s[M - k] = e - cmul(conjg(w), o);
+        s[(M - k) * ES] = e - cmul(conjg(w), o);
     }
 }
 
 // Row pass over (z, y) rows of W.  Persistent CTAs walk tiles of ROWS
-// consecutive rows; each tile's rows are contiguous in HBM and are streamed
-// with cp.async into a staging buffer (two, alternating) while the previous
-// tile is transformed.  Pencils (b*3*ROWS + r*3 + c) of length PL = N/2+2
-// hold the transposed rows for the FFTs.
+// consecutive rows; a tile's rows are contiguous in HBM and are streamed
+// with cp.async into one of two staging buffers while the previous tile is
+// transformed.  The FFTs run in place on the interleaved rows: the pencil of
+// component c of row r of buffer b starts at ((b*ROWS + r)*RL + c) with
+// element stride 3.
 template <typename T, int N, int MODE>
 __device__ __forceinline__ void row_issue_load(cpx<T>* stage, const cpx<T>* wu, const cpx<T>* ww,
-                                               const T* rin, size_t row0, size_t nxp3, int tid) {
+                                               const T* rin, size_t row0, int tid) {
     constexpr int ROWS = row_rows<T, N, MODE>();
     constexpr int VPE = 16 / (int)sizeof(cpx<T>);
     if constexpr (MODE == RM_R2C) {
@@ -486,7 +537,7 @@ __device__ __forceinline__ void row_issue_load(cpx<T>* stage, const cpx<T>* wu, 
         for (int e = tid; e < NBIN * NV; e += ROW_THREADS) {
             const int v = e % NV;
             const int b = e / NV;
-            const cpx<T>* src = ((b == 0) ? wu : ww) + row0 * nxp3;
+            const cpx<T>* src = ((b == 0) ? wu : ww) + row0 * RL;
             cp_async16(&stage[b * ROWS * RL + v * VPE], &src[v * VPE]);
         }
     }
@@ -499,30 +550,35 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
          const cpx<T>* __restrict__ tw_g, int ntiles) {
     constexpr int M = N / 2;
     constexpr int ROWS = row_rows<T, N, MODE>();
-    constexpr int PL = row_pl<N>();
     constexpr int RL = row_rl<N>();
     constexpr int NBIN = (MODE == RM_NONLIN) ? 2 : 1;
+    constexpr int VPE = 16 / (int)sizeof(cpx<T>);
     constexpr int STAGE = (MODE == RM_R2C) ? ROWS * N * 3 / 2 : ROWS * NBIN * RL;
+    using LI = Lay<3, RL, 1, 3>;  // interleaved rows
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* stage0 = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* S = stage0 + 2 * STAGE;
-    cpx<T>* tw = S + (MODE == RM_NONLIN ? 6 : 3) * ROWS * PL;
+    cpx<T>* pen = stage0 + 2 * STAGE;                          // R2C only
+    cpx<T>* tw = pen + ((MODE == RM_R2C) ? ROWS * RL : 0);
+    int* posn = reinterpret_cast<int*>(tw + N);                // DIF position of frequency n
     const int tid = threadIdx.x;
-    const int nxv = kp.nxv;
-    const size_t nxp3 = (size_t)kp.nxp * 3;
 
     for (int i = tid; i < N; i += ROW_THREADS) tw[i] = tw_g[i];
+    for (int i = tid; i < M; i += ROW_THREADS) posn[i] = dif_position<M>(i);
+    if constexpr (MODE == RM_R2C) {
+        // padding columns of the output rows are written out: start them at 0
+        for (int i = tid; i < ROWS * RL; i += ROW_THREADS) pen[i] = zero_c<T>();
+    }
 
     int t = blockIdx.x;
-    if (t < ntiles) row_issue_load<T, N, MODE>(stage0, wu, ww, rin, (size_t)t * ROWS, nxp3, tid);
+    if (t < ntiles) row_issue_load<T, N, MODE>(stage0, wu, ww, rin, (size_t)t * ROWS, tid);
     cp_async_commit();
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
-        const cpx<T>* stage = stage0 + (it & 1) * STAGE;
+        cpx<T>* S = stage0 + (it & 1) * STAGE;
         {
             const int tn = t + gridDim.x;
             if (tn < ntiles)
                 row_issue_load<T, N, MODE>(stage0 + ((it + 1) & 1) * STAGE, wu, ww, rin,
-                                           (size_t)tn * ROWS, nxp3, tid);
+                                           (size_t)tn * ROWS, tid);
             cp_async_commit();
         }
         cp_async_wait<1>();
@@ -530,47 +586,36 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
         const size_t row0 = (size_t)t * ROWS;
 
         if constexpr (MODE == RM_R2C) {
-            // real rows into digit-reversed complex pencils z[n] = (x[2n], x[2n+1])
-            const T* rs = reinterpret_cast<const T*>(stage);
+            // real rows -> digit-reversed complex pencils z_c[n] = (x[2n][c], x[2n+1][c])
+            const T* rs = reinterpret_cast<const T*>(S);
             for (int e = tid; e < ROWS * 3 * M; e += ROW_THREADS) {
                 const int c = e % 3;
                 const int r2 = e / 3;
                 const int n = r2 % M;
                 const int r = r2 / M;
-                const T* src = rs + ((size_t)r * N + 2 * n) * 3 + c;
-                S[(r * 3 + c) * PL + dif_position<M>(n)] = mk<T>(src[0], src[3]);
+                const T* src = rs + (r * N + 2 * n) * 3 + c;
+                pen[r * RL + posn[n] * 3 + c] = mk<T>(src[0], src[3]);
             }
             __syncthreads();
         } else {
-            // transpose [r][kx][c] -> pencils [b][r][c][kx], kx fastest
-            // (staging read at stride 3, pencil write at stride 1)
-            for (int e = tid; e < ROWS * NBIN * 3 * nxv; e += ROW_THREADS) {
-                const int kx = e % nxv;
-                const int p = e / nxv;  // = b*3*ROWS + r*3 + c
-                const int c = p % 3;
-                const int r = (p / 3) % ROWS;
-                const int b = p / (3 * ROWS);
-                S[p * PL + kx] = stage[(b * ROWS + r) * RL + kx * 3 + c];
-            }
-            __syncthreads();
             constexpr int NP = NBIN * 3 * ROWS;
             for (int e = tid; e < NP * (M / 2 + 1); e += ROW_THREADS) {
                 const int k = e % (M / 2 + 1);
                 const int p = e / (M / 2 + 1);
-                c2r_pre<T, N>(S + p * PL, tw, k);
+                c2r_pre<T, N, 3>(S + LI::base(p), tw, k);
             }
             __syncthreads();
-            dif<T, M, true, NP, PL, 1, 2, N>(S, tw, tid, ROW_THREADS);
+            dif<T, M, true, NP, LI, 2, N>(S, tw, tid, ROW_THREADS);
 
             if constexpr (MODE == RM_C2R || WRITE_RU) {
-                // real u (first 3*ROWS pencils) to rout, natural x order
+                // real u (buffer 0) to rout in natural x order
                 for (int e = tid; e < ROWS * N * 3; e += ROW_THREADS) {
                     const int c = e % 3;
                     const int r2 = e / 3;
                     const int x = r2 % N;
                     const int r = r2 / N;
-                    const cpx<T> z = S[(r * 3 + c) * PL + dif_position<M>(x >> 1)];
-                    rout[((row0 + r) * N + x) * 3 + c] = (x & 1) ? z.y : z.x;
+                    const cpx<T> z = S[r * RL + posn[x >> 1] * 3 + c];
+                    rout[(row0 + r) * (N * 3) + x * 3 + c] = (x & 1) ? z.y : z.x;
                 }
             }
             if constexpr (MODE == RM_C2R) {
@@ -584,36 +629,40 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
                 for (int e = tid; e < ROWS * M; e += ROW_THREADS) {
                     const int p = e % M;
                     const int r = e / M;
+                    cpx<T>* up = S + r * RL + p * 3;
+                    const cpx<T>* wp = S + (ROWS + r) * RL + p * 3;
                     cpx<T> u[3], w[3];
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        u[c] = S[(r * 3 + c) * PL + p];
-                        w[c] = S[(3 * ROWS + r * 3 + c) * PL + p];
+                        u[c] = up[c];
+                        w[c] = wp[c];
                     }
 #pragma unroll
                     for (int cc = 0; cc < 3; ++cc) {
                         const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
                         const T tx = u[c1].x * w[c2].x - u[c2].x * w[c1].x;
                         const T ty = u[c1].y * w[c2].y - u[c2].y * w[c1].y;
-                        S[(r * 3 + cc) * PL + p] = mk<T>(tx * inv_np, ty * inv_np);
+                        up[cc] = mk<T>(tx * inv_np, ty * inv_np);
                     }
                 }
                 __syncthreads();
             }
         }
         // forward: digit-reversed -> natural, then R2C post-processing
-        dit<T, M, false, 3 * ROWS, PL, 1, 2, N>(S, tw, tid, ROW_THREADS);
+        cpx<T>* F = (MODE == RM_R2C) ? pen : S;
+        dit<T, M, false, 3 * ROWS, LI, 2, N>(F, tw, tid, ROW_THREADS);
         for (int e = tid; e < 3 * ROWS * (M / 2 + 1); e += ROW_THREADS) {
             const int k = e % (M / 2 + 1);
             const int p = e / (M / 2 + 1);
-            r2c_post<T, N>(S + p * PL, tw, k);
+            r2c_post<T, N, 3>(F + LI::base(p), tw, k);
         }
         __syncthreads();
-        for (int e = tid; e < ROWS * nxv * 3; e += ROW_THREADS) {
-            const int q = e % (nxv * 3);
-            const int r = e / (nxv * 3);
-            const int kx = q / 3, c = q % 3;
-            wout[(row0 + r) * nxp3 + q] = S[(r * 3 + c) * PL + kx];
+        // padded rows out (padding columns carry zeros), 16-byte vectors
+        {
+            using V = float4;
+            const V* src = reinterpret_cast<const V*>(F);
+            V* dst = reinterpret_cast<V*>(wout + row0 * RL);
+            for (int v = tid; v < ROWS * RL / VPE; v += ROW_THREADS) dst[v] = src[v];
         }
         __syncthreads();
     }
