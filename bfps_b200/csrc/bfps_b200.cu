@@ -210,7 +210,7 @@ struct Engine {
                    void* out1, const void* v0 = nullptr, const void* vp = nullptr,
                    const void* fsrc = nullptr) {
         constexpr int NB = col_nb(MODE);
-        constexpr int TKX = col_tkx<T, N, NB>();
+        constexpr int TKX = col_tkx<T, N, MODE>();
         constexpr size_t smem = col_smem_bytes<T, N, MODE>();
         auto kern = col_pass<T, N, MODE>;
         if (smem > (size_t)c->smem_optin)
@@ -501,11 +501,11 @@ static int ensure_ru(bfg_ctx* c) {
 // ----------------------------------------------------------- tracers --
 template <typename T, int NB, int MM>
 static int launch_tracers(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out) {
-    const unsigned blocks = (unsigned)((p->n + 127) / 128);
+    const unsigned blocks = (unsigned)((p->n + TRACER_THREADS - 1) / TRACER_THREADS);
     if (blocks == 0) return 0;
     Prof pr(c, K_TRACER);
-    tracer_kernel<T, NB, MM><<<blocks, 128, 0, c->stream>>>(pp, (const T*)c->ru, p->pos, p->hist,
-                                                           out);
+    tracer_kernel<T, NB, MM><<<blocks, TRACER_THREADS, 0, c->stream>>>(
+        pp, (const T*)c->ru, p->pos, p->hist, out);
     return after_launch(c, "tracer_kernel");
 }
 

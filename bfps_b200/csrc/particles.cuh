@@ -116,8 +116,10 @@ __device__ __forceinline__ void row_accumulate(const T* __restrict__ row, int x0
     }
 }
 
+constexpr int TRACER_THREADS = 128;
+
 template <typename T, int NB, int MM>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(TRACER_THREADS)
 tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ pos,
               double* __restrict__ hist, double* __restrict__ sample_out) {
     constexpr int NP = 2 * NB + 2;

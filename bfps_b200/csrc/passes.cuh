@@ -70,29 +70,34 @@ template <typename T, int NB>
 __host__ __device__ constexpr int col_pitch_for(int tkx) {
     return NB * 3 * tkx + (sizeof(T) == 4 ? 2 : 1);
 }
-template <typename T, int N, int NB>
+// number of RK operand arrays streamed with the tile (FZ passes)
+__host__ __device__ constexpr int col_nrk(int mode) {
+    return mode == CM_FZ_RK1 ? 1 : ((mode == CM_FZ_RK2 || mode == CM_FZ_RK3) ? 2 : 0);
+}
+// two tile buffers + the RK operand tile + twiddles
+template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t col_bytes_for(int tkx) {
-    return (size_t)(2 * N * col_pitch_for<T, NB>(tkx) + N) * sizeof(cpx<T>);
+    return (size_t)(2 * N * col_pitch_for<T, col_nb(MODE)>(tkx) + col_nrk(MODE) * N * 3 * tkx + N) *
+           sizeof(cpx<T>);
 }
-// kx columns per tile: the widest power of two (<= 16) whose two tile
-// buffers fit the shared-memory budget
-template <typename T, int N, int NB>
+// kx columns per tile: the widest power of two (<= 16) that fits the budget
+template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_tkx_from(int tkx) {
-    return (tkx <= 1 || col_bytes_for<T, N, NB>(tkx) <= (size_t)SMEM_BUDGET)
+    return (tkx <= 1 || col_bytes_for<T, N, MODE>(tkx) <= (size_t)SMEM_BUDGET)
                ? tkx
-               : col_tkx_from<T, N, NB>(tkx / 2);
+               : col_tkx_from<T, N, MODE>(tkx / 2);
 }
-template <typename T, int N, int NB>
+template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_tkx() {
-    return col_tkx_from<T, N, NB>(16);
+    return col_tkx_from<T, N, MODE>(16);
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_pitch() {
-    return col_pitch_for<T, col_nb(MODE)>(col_tkx<T, N, col_nb(MODE)>());
+    return col_pitch_for<T, col_nb(MODE)>(col_tkx<T, N, MODE>());
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t col_smem_bytes() {
-    return col_bytes_for<T, N, col_nb(MODE)>(col_tkx<T, N, col_nb(MODE)>());
+    return col_bytes_for<T, N, MODE>(col_tkx<T, N, MODE>());
 }
 
 template <int N>
@@ -244,7 +249,7 @@ __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
                                                size_t nxp3, int tid) {
     constexpr int NB = col_nb(MODE);
     constexpr int NBIN = col_nbin(MODE);
-    constexpr int TKX = col_tkx<T, N, NB>();
+    constexpr int TKX = col_tkx<T, N, MODE>();
     constexpr int W = 3 * TKX;
     constexpr int PR = col_pitch<T, N, MODE>();
     constexpr int VB = ((W * (int)sizeof(cpx<T>)) % 16 == 0) ? 16 : 8;
@@ -272,7 +277,7 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
          const T* __restrict__ filt, const T* __restrict__ fac,
          const cpx<T>* __restrict__ tw_g, int ntx, int ntiles) {
     constexpr int NB = col_nb(MODE);
-    constexpr int TKX = col_tkx<T, N, NB>();
+    constexpr int TKX = col_tkx<T, N, MODE>();
     constexpr int W = 3 * TKX;                     // complex per row per buffer
     constexpr int PR = col_pitch<T, N, MODE>();    // tile row pitch
     constexpr int TILE = N * PR;
@@ -281,9 +286,11 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
     constexpr int VPE = VB / (int)sizeof(cpx<T>) > 0 ? VB / (int)sizeof(cpx<T>) : 1;
     constexpr int WV = W / VPE;
     using V = typename vec_of<VB>::type;
+    constexpr int NRK = col_nrk(MODE);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* bufs = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* tw = bufs + 2 * TILE;
+    cpx<T>* rkt = bufs + 2 * TILE;        // RK operand tile [arr][l][W] (FZ passes)
+    cpx<T>* tw = rkt + NRK * N * W;
 
     const int tid = threadIdx.x;
     const size_t nxp3 = (size_t)kp.nxp * 3;
@@ -297,35 +304,35 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
     cp_async_commit();
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
         cpx<T>* tile = bufs + (it & 1) * TILE;
+        if constexpr (NRK > 0) {
+            // RK operands of this tile: rows S[ky=a][kz=l], streamed while the
+            // tile is transformed (the epilogue of the previous tile is done)
+            const int a = t / ntx;
+            const int kx0 = (t % ntx) * TKX;
+            const int nvalid = (3 * min(TKX, kp.nxv - kx0) + VPE - 1) / VPE;
+            for (int e = tid; e < N * NRK * WV; e += COL_THREADS) {
+                const int v = e % WV;
+                const int r = e / WV;
+                const int arr = r % NRK;
+                const int l = r / NRK;
+                if (v >= nvalid) continue;
+                const cpx<T>* src = ((arr == 0) ? rk_v0 : rk_vp) + ((size_t)a * N + l) * nxp3 +
+                                    (size_t)kx0 * 3 + v * VPE;
+                cp_async<VB>(&rkt[(arr * N + l) * W + v * VPE], src);
+            }
+            cp_async_commit();
+        }
         {
             const int tn = t + gridDim.x;
             if (tn < ntiles) {
                 const int kx0n = (tn % ntx) * TKX;
                 col_issue_load<T, N, MODE>(bufs + ((it + 1) & 1) * TILE, in0, in1, tn / ntx, kx0n,
                                            min(TKX, kp.nxv - kx0n), nxp3, tid);
-                if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
-                    // RK operands of the next tile into L2 while this tile is transformed
-                    constexpr int LINES = (W * (int)sizeof(cpx<T>) + 127) / 128 + 1;
-                    constexpr int NARR = (MODE == CM_FZ_RK1) ? 1 : 2;
-                    const int an = tn / ntx;
-                    for (int e = tid; e < N * NARR * LINES; e += COL_THREADS) {
-                        const int ln = e % LINES;
-                        const int r = e / LINES;
-                        const int arr = r % NARR;
-                        const int l = r / NARR;
-                        const char* base = reinterpret_cast<const char*>(
-                            ((arr == 0) ? rk_v0 : rk_vp) + ((size_t)an * N + l) * nxp3 +
-                            (size_t)kx0n * 3);
-                        const char* a0 = reinterpret_cast<const char*>(
-                            reinterpret_cast<uintptr_t>(base) & ~(uintptr_t)127);
-                        const char* pl = a0 + ln * 128;
-                        if (pl < base + W * (int)sizeof(cpx<T>)) prefetch_l2(pl);
-                    }
-                }
             }
             cp_async_commit();
         }
-        cp_async_wait<1>();
+        if constexpr (NRK > 0) cp_async_wait<2>();
+        else cp_async_wait<1>();
         __syncthreads();
         const int a = t / ntx;
         const int kx0 = (t % ntx) * TKX;
@@ -365,38 +372,19 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
         constexpr int NST = plan_nstages(N);
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
             dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, COL_THREADS);
-            // ---- epilogue: per point, two points per batch so that the RK
-            // operand loads of both are in flight together
+            cp_async_wait<1>();  // RK operand tile of this tile
+            __syncthreads();
+            // ---- epilogue: one thread per mode (kz = l, kx = kx0 + col)
             const double ky = kwrap<N>(a, kp.dky);
-            for (int e0 = tid; e0 < N * TKX; e0 += 2 * COL_THREADS) {
-                cpx<T> v0[2][3], vp[2][3];
-                size_t pt[2];
-                bool ok[2];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int e = e0 + h * COL_THREADS;
-                    const int col = e % TKX;
-                    const int l = e / TKX;
-                    ok[h] = e < N * TKX && col < ncol;
-                    pt[h] = ((size_t)a * N + l) * kp.nxp + kx0 + col;  // S[ky=a][kz=l][kx]
-                    if (ok[h]) {
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) v0[h][c] = rk_v0[pt[h] * 3 + c];
-                        if (MODE != CM_FZ_RK1) {
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) vp[h][c] = rk_vp[pt[h] * 3 + c];
-                        }
-                    }
-                }
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    if (!ok[h]) continue;
-                    const int e = e0 + h * COL_THREADS;
-                    const int col = e % TKX;
-                    const int l = e / TKX;  // output kz index
-                    fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, ky, v0[h], vp[h],
-                                         pt[h], filt, fac, fsrc, out0);
-                }
+            for (int e = tid; e < N * TKX; e += COL_THREADS) {
+                const int col = e % TKX;
+                const int l = e / TKX;
+                if (col >= ncol) continue;
+                const size_t pt = ((size_t)a * N + l) * kp.nxp + kx0 + col;  // S[ky=a][kz=l][kx]
+                const cpx<T>* v0 = &rkt[l * W + col * 3];
+                const cpx<T>* vp = &rkt[((NRK - 1) * N + l) * W + col * 3];
+                fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, ky, v0, vp, pt, filt,
+                                     fac, fsrc, out0);
             }
         } else {
             dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, COL_THREADS);
@@ -437,14 +425,18 @@ constexpr int ROW_THREADS = 512;
 
 template <int N>
 __host__ __device__ constexpr int row_rl() { return (N / 2 + 4) * 3; }  // padded row, complex
-// shared memory for R rows: staging (two alternating buffers; the FFTs run in
-// place on the interleaved [kx][c] rows), twiddles, digit-reversal table
+template <int N>
+__host__ __device__ constexpr int row_pl() { return N / 2 + 1; }  // odd pencil pitch
+// shared memory for R rows: staging (two alternating buffers of interleaved
+// rows as they sit in HBM), pencils (one per component, odd pitch), output
+// rows (R2C only), twiddles and the digit-reversal table
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t row_bytes_for(int R) {
-    return (MODE == RM_R2C)
-               ? (size_t)(2 * R * (N * 3 / 2) + R * row_rl<N>() + N) * sizeof(cpx<T>) + (N / 2) * 4
-               : (size_t)(2 * R * (MODE == RM_NONLIN ? 2 : 1) * row_rl<N>() + N) * sizeof(cpx<T>) +
-                     (N / 2) * 4;
+    return (size_t)((MODE == RM_R2C) ? 2 * R * (N * 3 / 2) + R * row_rl<N>()
+                                     : 2 * R * (MODE == RM_NONLIN ? 2 : 1) * row_rl<N>()) *
+               sizeof(cpx<T>) +
+           (size_t)((MODE == RM_NONLIN ? 6 : 3) * R * row_pl<N>() + N) * sizeof(cpx<T>) +
+           (size_t)(N / 2) * 4;
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int row_rows_from(int R) {
@@ -461,66 +453,70 @@ __host__ __device__ constexpr size_t row_smem_bytes() {
     return row_bytes_for<T, N, MODE>(row_rows<T, N, MODE>());
 }
 
-// C2R pre-processing of one pencil (element stride ES): pairs (k, M-k),
-// X[0] and X[M] enter with their real parts only.
-template <typename T, int N, int ES>
-__device__ __forceinline__ void c2r_pre(cpx<T>* s, const cpx<T>* tw, int k) {
+// C2R pre-processing (pairs k, M-k; X[0] and X[M] enter with their real
+// parts only), reading X from an interleaved row (stride 3) and writing Z to
+// a contiguous pencil.
+template <typename T, int N>
+__device__ __forceinline__ void c2r_pre(const cpx<T>* x, cpx<T>* z, const cpx<T>* tw, int k) {
     constexpr int M = N / 2;
     if (k == 0) {
-        const T x0 = s[0].x, xm = s[M * ES].x;
-        s[0] = mk<T>(x0 + xm, x0 - xm);
+        const T x0 = x[0].x, xm = x[3 * M].x;
+        z[0] = mk<T>(x0 + xm, x0 - xm);
         return;
     }
-    const cpx<T> a = s[k * ES], b = s[(M - k) * ES];
+    const cpx<T> a = x[3 * k], b = x[3 * (M - k)];
     const cpx<T> w = tw[k];  // exp(-2 pi i k / N)
     // Z[k] = (a + conj b) + i conj(w) (a - conj b)
     {
         const cpx<T> sp = a + conjg(b), dm = a - conjg(b);
         const cpx<T> e = cmulc(dm, w);  // dm * conj(w)
-        s[k * ES] = mk<T>(sp.x - e.y, sp.y + e.x);
+        z[k] = mk<T>(sp.x - e.y, sp.y + e.x);
     }
     if (k != M - k) {
         // Z[M-k] = (b + conj a) - i w (b - conj a)
         const cpx<T> sp = b + conjg(a), dm = b - conjg(a);
         const cpx<T> e = cmul(dm, w);
-        s[(M - k) * ES] = mk<T>(sp.x + e.y, sp.y - e.x);
+        z[M - k] = mk<T>(sp.x + e.y, sp.y - e.x);
     }
 }
 
-// R2C post-processing of one pencil (natural-order Z), writes X[0..M].
-template <typename T, int N, int ES>
-__device__ __forceinline__ void r2c_post(cpx<T>* s, const cpx<T>* tw, int k) {
+// R2C post-processing: natural-order Z from a contiguous pencil, X[0..M]
+// written into an interleaved row (stride 3).
+template <typename T, int N>
+__device__ __forceinline__ void r2c_post(const cpx<T>* z, cpx<T>* x, const cpx<T>* tw, int k) {
     constexpr int M = N / 2;
     const T h = (T)0.5;
     if (k == 0) {
-        const cpx<T> z0 = s[0];
-        s[0] = mk<T>(z0.x + z0.y, (T)0);
-        s[M * ES] = mk<T>(z0.x - z0.y, (T)0);
+        const cpx<T> z0 = z[0];
+        x[0] = mk<T>(z0.x + z0.y, (T)0);
+        x[3 * M] = mk<T>(z0.x - z0.y, (T)0);
         return;
     }
-    const cpx<T> zk = s[k * ES], zm = s[(M - k) * ES];
+    const cpx<T> zk = z[k], zm = z[M - k];
     const cpx<T> w = tw[k];
     {
         const cpx<T> e = scale(zk + conjg(zm), h);
         const cpx<T> d = zk - conjg(zm);
         const cpx<T> o = mk<T>(d.y * h, -d.x * h);  // d / (2i)
-        s[k * ES] = e + cmul(w, o);
+        x[3 * k] = e + cmul(w, o);
     }
     if (k != M - k) {
         // exp(-2 pi i (M-k)/N) = -conj(w)
         const cpx<T> e = scale(zm + conjg(zk), h);
         const cpx<T> d = zm - conjg(zk);
         const cpx<T> o = mk<T>(d.y * h, -d.x * h);
-        s[(M - k) * ES] = e - cmul(conjg(w), o);
+        x[3 * (M - k)] = e - cmul(conjg(w), o);
     }
 }
 
 // Row pass over (z, y) rows of W.  Persistent CTAs walk tiles of ROWS
 // consecutive rows; a tile's rows are contiguous in HBM and are streamed
 // with cp.async into one of two staging buffers while the previous tile is
-// transformed.  The FFTs run in place on the interleaved rows: the pencil of
-// component c of row r of buffer b starts at ((b*ROWS + r)*RL + c) with
-// element stride 3.
+// transformed.  The C2R pre-processing moves each component of each row into
+// its own pencil (odd pitch PL, so that lanes on consecutive pencils or
+// consecutive elements hit distinct banks); the R2C post-processing moves the
+// result back into the interleaved staging rows, which are stored with
+// 16-byte vectors.
 template <typename T, int N, int MODE>
 __device__ __forceinline__ void row_issue_load(cpx<T>* stage, const cpx<T>* wu, const cpx<T>* ww,
                                                const T* rin, size_t row0, int tid) {
@@ -551,29 +547,32 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
     constexpr int M = N / 2;
     constexpr int ROWS = row_rows<T, N, MODE>();
     constexpr int RL = row_rl<N>();
+    constexpr int PL = row_pl<N>();
     constexpr int NBIN = (MODE == RM_NONLIN) ? 2 : 1;
     constexpr int VPE = 16 / (int)sizeof(cpx<T>);
     constexpr int STAGE = (MODE == RM_R2C) ? ROWS * N * 3 / 2 : ROWS * NBIN * RL;
-    using LI = Lay<3, RL, 1, 3>;  // interleaved rows
+    constexpr int NP = NBIN * 3 * ROWS;  // pencils of the inverse transform
+    using LP = Lay<1, PL, 0, 1>;          // contiguous pencils, odd pitch
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* stage0 = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* pen = stage0 + 2 * STAGE;                          // R2C only
-    cpx<T>* tw = pen + ((MODE == RM_R2C) ? ROWS * RL : 0);
-    int* posn = reinterpret_cast<int*>(tw + N);                // DIF position of frequency n
+    cpx<T>* outr = stage0 + 2 * STAGE;                               // R2C output rows
+    cpx<T>* S = outr + ((MODE == RM_R2C) ? ROWS * RL : 0);           // pencils
+    cpx<T>* tw = S + ((MODE == RM_NONLIN) ? 6 : 3) * ROWS * PL;
+    int* posn = reinterpret_cast<int*>(tw + N);                      // DIF position of n
     const int tid = threadIdx.x;
 
     for (int i = tid; i < N; i += ROW_THREADS) tw[i] = tw_g[i];
     for (int i = tid; i < M; i += ROW_THREADS) posn[i] = dif_position<M>(i);
     if constexpr (MODE == RM_R2C) {
         // padding columns of the output rows are written out: start them at 0
-        for (int i = tid; i < ROWS * RL; i += ROW_THREADS) pen[i] = zero_c<T>();
+        for (int i = tid; i < ROWS * RL; i += ROW_THREADS) outr[i] = zero_c<T>();
     }
 
     int t = blockIdx.x;
     if (t < ntiles) row_issue_load<T, N, MODE>(stage0, wu, ww, rin, (size_t)t * ROWS, tid);
     cp_async_commit();
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
-        cpx<T>* S = stage0 + (it & 1) * STAGE;
+        cpx<T>* st = stage0 + (it & 1) * STAGE;
         {
             const int tn = t + gridDim.x;
             if (tn < ntiles)
@@ -587,34 +586,33 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
 
         if constexpr (MODE == RM_R2C) {
             // real rows -> digit-reversed complex pencils z_c[n] = (x[2n][c], x[2n+1][c])
-            const T* rs = reinterpret_cast<const T*>(S);
+            const T* rs = reinterpret_cast<const T*>(st);
             for (int e = tid; e < ROWS * 3 * M; e += ROW_THREADS) {
-                const int c = e % 3;
-                const int r2 = e / 3;
-                const int n = r2 % M;
-                const int r = r2 / M;
+                const int n = e % M;
+                const int p = e / M;  // = r*3 + c
+                const int c = p % 3, r = p / 3;
                 const T* src = rs + (r * N + 2 * n) * 3 + c;
-                pen[r * RL + posn[n] * 3 + c] = mk<T>(src[0], src[3]);
+                S[p * PL + posn[n]] = mk<T>(src[0], src[3]);
             }
             __syncthreads();
         } else {
-            constexpr int NP = NBIN * 3 * ROWS;
+            // C2R pre-processing, interleaved rows -> pencils
             for (int e = tid; e < NP * (M / 2 + 1); e += ROW_THREADS) {
                 const int k = e % (M / 2 + 1);
-                const int p = e / (M / 2 + 1);
-                c2r_pre<T, N, 3>(S + LI::base(p), tw, k);
+                const int p = e / (M / 2 + 1);  // = (b*ROWS + r)*3 + c
+                c2r_pre<T, N>(st + (p / 3) * RL + (p % 3), S + p * PL, tw, k);
             }
             __syncthreads();
-            dif<T, M, true, NP, LI, 2, N>(S, tw, tid, ROW_THREADS);
+            dif<T, M, true, NP, LP, 2, N>(S, tw, tid, ROW_THREADS);
 
             if constexpr (MODE == RM_C2R || WRITE_RU) {
-                // real u (buffer 0) to rout in natural x order
+                // real u (pencils of buffer 0) to rout in natural x order
                 for (int e = tid; e < ROWS * N * 3; e += ROW_THREADS) {
                     const int c = e % 3;
                     const int r2 = e / 3;
                     const int x = r2 % N;
                     const int r = r2 / N;
-                    const cpx<T> z = S[r * RL + posn[x >> 1] * 3 + c];
+                    const cpx<T> z = S[(r * 3 + c) * PL + posn[x >> 1]];
                     rout[(row0 + r) * (N * 3) + x * 3 + c] = (x & 1) ? z.y : z.x;
                 }
             }
@@ -629,39 +627,37 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
                 for (int e = tid; e < ROWS * M; e += ROW_THREADS) {
                     const int p = e % M;
                     const int r = e / M;
-                    cpx<T>* up = S + r * RL + p * 3;
-                    const cpx<T>* wp = S + (ROWS + r) * RL + p * 3;
                     cpx<T> u[3], w[3];
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        u[c] = up[c];
-                        w[c] = wp[c];
+                        u[c] = S[(r * 3 + c) * PL + p];
+                        w[c] = S[(3 * ROWS + r * 3 + c) * PL + p];
                     }
 #pragma unroll
                     for (int cc = 0; cc < 3; ++cc) {
                         const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
                         const T tx = u[c1].x * w[c2].x - u[c2].x * w[c1].x;
                         const T ty = u[c1].y * w[c2].y - u[c2].y * w[c1].y;
-                        up[cc] = mk<T>(tx * inv_np, ty * inv_np);
+                        S[(r * 3 + cc) * PL + p] = mk<T>(tx * inv_np, ty * inv_np);
                     }
                 }
                 __syncthreads();
             }
         }
-        // forward: digit-reversed -> natural, then R2C post-processing
-        cpx<T>* F = (MODE == RM_R2C) ? pen : S;
-        dit<T, M, false, 3 * ROWS, LI, 2, N>(F, tw, tid, ROW_THREADS);
+        // forward: digit-reversed -> natural, then R2C post-processing into
+        // interleaved rows (the staging rows of u, or the R2C output rows)
+        dit<T, M, false, 3 * ROWS, LP, 2, N>(S, tw, tid, ROW_THREADS);
+        cpx<T>* orow = (MODE == RM_R2C) ? outr : st;
         for (int e = tid; e < 3 * ROWS * (M / 2 + 1); e += ROW_THREADS) {
             const int k = e % (M / 2 + 1);
-            const int p = e / (M / 2 + 1);
-            r2c_post<T, N, 3>(F + LI::base(p), tw, k);
+            const int p = e / (M / 2 + 1);  // = r*3 + c
+            r2c_post<T, N>(S + p * PL, orow + (p / 3) * RL + (p % 3), tw, k);
         }
         __syncthreads();
         // padded rows out (padding columns carry zeros), 16-byte vectors
         {
-            using V = float4;
-            const V* src = reinterpret_cast<const V*>(F);
-            V* dst = reinterpret_cast<V*>(wout + row0 * RL);
+            const float4* src = reinterpret_cast<const float4*>(orow);
+            float4* dst = reinterpret_cast<float4*>(wout + row0 * RL);
             for (int v = tid; v < ROWS * RL / VPE; v += ROW_THREADS) dst[v] = src[v];
         }
         __syncthreads();
