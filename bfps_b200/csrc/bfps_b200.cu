@@ -53,6 +53,8 @@ struct bfg_ctx {
     int nfilt = 1;
     void* fac = nullptr;
     double fac_dt = NAN, fac_nu = NAN;
+    void* dmember = nullptr;   // this context as a one-element Member<T> array
+    std::vector<unsigned char> hmember;  // last uploaded copy
     void* stats_ws = nullptr;  // statistics partial sums
     size_t stats_ws_bytes = 0;
     size_t field_bytes = 0;
@@ -204,72 +206,80 @@ static double kwrap_h(int i, int N, double dk) { return dk * (double)(i <= N / 2
 template <typename T, int N>
 struct Engine {
     using C = cpx<T>;
+    using Mem = Member<T>;
 
+    // one persistent launch of a column pass over nmem members
     template <int MODE>
-    static int col(bfg_ctx* c, double dt, const void* in0, const void* in1, void* out0,
-                   void* out1, const void* v0 = nullptr, const void* vp = nullptr,
-                   const void* fsrc = nullptr) {
-        constexpr int NB = col_nb(MODE);
+    static int col(bfg_ctx* c, const Mem* mem, int nmem, Roles rl) {
         constexpr int TKX = col_tkx<T, N, MODE>();
         constexpr size_t smem = col_smem_bytes<T, N, MODE>();
         auto kern = col_pass<T, N, MODE>;
         if (smem > (size_t)c->smem_optin)
             return fail(c, BFG_EUNSUP, "column pass needs %zu bytes of shared memory", smem);
         CU(ensure_smem(kern, smem, c->device));
-        const int ntx = (c->nxv + TKX - 1) / TKX;
-        const int ntiles = ntx * N;
+        const int ntx = (N / 2 + 1 + TKX - 1) / TKX;
+        const int tiles_per = ntx * N;
+        const int ntiles = tiles_per * nmem;
         const int grid = std::min(ntiles, c->nsm);
         constexpr int kind = (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) ? K_IZ
                              : (MODE == CM_Y_INV1 || MODE == CM_Y_INV2)                  ? K_IY
                              : (MODE == CM_Y_FWD1)                                      ? K_FY
                                                                                         : K_FZ;
         Prof pr(c, kind);
-        kern<<<grid, COL_THREADS, smem, c->stream>>>(
-            kparams(c, dt), (const C*)in0, (const C*)in1, (C*)out0, (C*)out1, (const C*)v0,
-            (const C*)vp, (const C*)fsrc, (const T*)c->filt, (const T*)c->fac,
-            (const C*)c->tw, ntx, ntiles);
+        kern<<<grid, COL_THREADS, smem, c->stream>>>(mem, rl, (const C*)c->tw, ntx, tiles_per,
+                                                     ntiles);
         return after_launch(c, "col_pass");
     }
 
+    // one persistent launch of a row pass over nmem members
     template <int MODE, bool WRU>
-    static int row(bfg_ctx* c, const void* wu, const void* ww, void* wout, void* rout,
-                   const void* rin) {
+    static int row(bfg_ctx* c, const Mem* mem, int nmem, Roles rl) {
         constexpr size_t smem = row_smem_bytes<T, N, MODE>();
         constexpr int ROWS = row_rows<T, N, MODE>();
         auto kern = row_pass<T, N, MODE, WRU>;
         if (smem > (size_t)c->smem_optin)
             return fail(c, BFG_EUNSUP, "row pass needs %zu bytes of shared memory", smem);
         CU(ensure_smem(kern, smem, c->device));
-        const int ntiles = N * N / ROWS;
+        const int tiles_per = N * N / ROWS;
+        const int ntiles = tiles_per * nmem;
         const int grid = std::min(ntiles, c->nsm);
         Prof pr(c, K_X);
-        row_pass<T, N, MODE, WRU><<<grid, ROW_THREADS, smem, c->stream>>>(
-            kparams(c, 0.0), (const C*)wu, (const C*)ww, (C*)wout, (T*)rout, (const T*)rin,
-            (const C*)c->tw, ntiles);
+        kern<<<grid, ROW_THREADS, smem, c->stream>>>(mem, rl, (const C*)c->tw, tiles_per, ntiles);
         return after_launch(c, "row_pass");
     }
 
-    static int symmetrize(bfg_ctx* c, void* buf) {
+    static int symmetrize(bfg_ctx* c, const Mem* mem, int nmem, int bufi) {
         Prof pr(c, K_KSPACE);
-        symmetrize_kernel<T, N><<<(N * N + 255) / 256, 256, 0, c->stream>>>((C*)buf, c->nxp);
+        symmetrize_kernel<T, N><<<dim3((N * N + 255) / 256, nmem), 256, 0, c->stream>>>(mem, bufi);
         return after_launch(c, "symmetrize");
     }
 
-    static int stage(bfg_ctx* c, int s, double dt, bool write_ru) {
+    // RK stage s of every member: IZ -> IY -> X -> FY -> FZ (with update)
+    static int stage(bfg_ctx* c, const Mem* mem, int nmem, int s, bool write_ru) {
         int rc;
-        const void* src = s == 0 ? c->w0 : (s == 1 ? c->v1 : c->v2);
-        if ((rc = col<CM_IZ_VEL>(c, dt, src, nullptr, c->wa, c->wb))) return rc;
-        if ((rc = col<CM_Y_INV2>(c, dt, c->wa, c->wb, c->wa, c->wb))) return rc;
-        if (write_ru) rc = row<RM_NONLIN, true>(c, c->wa, c->wb, c->wa, c->ru, nullptr);
-        else rc = row<RM_NONLIN, false>(c, c->wa, c->wb, c->wa, nullptr, nullptr);
+        const int src = s == 0 ? B_W0 : (s == 1 ? B_V1 : B_V2);
+        if ((rc = col<CM_IZ_VEL>(c, mem, nmem, roles(src, B_NONE, B_WA, B_WB)))) return rc;
+        if ((rc = col<CM_Y_INV2>(c, mem, nmem, roles(B_WA, B_WB, B_WA, B_WB)))) return rc;
+        if (write_ru)
+            rc = row<RM_NONLIN, true>(c, mem, nmem, roles(B_WA, B_WB, B_WA, B_NONE, B_NONE, B_NONE,
+                                                          B_NONE, B_RU));
+        else
+            rc = row<RM_NONLIN, false>(c, mem, nmem, roles(B_WA, B_WB, B_WA, B_NONE));
         if (rc) return rc;
-        if ((rc = col<CM_Y_FWD1>(c, dt, c->wa, nullptr, c->wa, nullptr))) return rc;
-        if (s == 0) return col<CM_FZ_RK1>(c, dt, c->wa, nullptr, c->v1, nullptr, c->w0, nullptr, src);
-        if (s == 1) return col<CM_FZ_RK2>(c, dt, c->wa, nullptr, c->v2, nullptr, c->w0, c->v1, src);
-        return col<CM_FZ_RK3>(c, dt, c->wa, nullptr, c->w0, nullptr, c->w0, c->v2, src);
+        if ((rc = col<CM_Y_FWD1>(c, mem, nmem, roles(B_WA, B_NONE, B_WA, B_NONE)))) return rc;
+        if (s == 0)
+            return col<CM_FZ_RK1>(c, mem, nmem, roles(B_WA, B_NONE, B_V1, B_NONE, B_W0, B_NONE, src));
+        if (s == 1)
+            return col<CM_FZ_RK2>(c, mem, nmem, roles(B_WA, B_NONE, B_V2, B_NONE, B_W0, B_V1, src));
+        return col<CM_FZ_RK3>(c, mem, nmem, roles(B_WA, B_NONE, B_W0, B_NONE, B_W0, B_V2, src));
     }
 
-    static int finish_step(bfg_ctx* c) { return symmetrize(c, c->w0); }
+    static int finish_step(bfg_ctx* c, const Mem* mem, int nmem) {
+        return symmetrize(c, mem, nmem, B_W0);
+    }
+
+    // ---- single-context operations (the context's own member) -------------
+    static const Mem* self(bfg_ctx* c) { return (const Mem*)c->dmember; }
 
     static int velocity_state(bfg_ctx* c) {
         const size_t npts = (size_t)N * N * c->nxv;
@@ -278,18 +288,19 @@ struct Engine {
             kparams(c, 0.0), (const C*)c->w0, (C*)c->wa);
         int rc = after_launch(c, "velocity");
         if (rc) return rc;
-        return symmetrize(c, c->wa);
+        return symmetrize(c, self(c), 1, B_WA);
     }
 
     static int velocity_rspace(bfg_ctx* c) {
         int rc;
-        if ((rc = col<CM_IZ_U>(c, 0.0, c->w0, nullptr, c->wb, nullptr))) return rc;
-        if ((rc = col<CM_Y_INV1>(c, 0.0, c->wb, nullptr, c->wb, nullptr))) return rc;
-        return row<RM_C2R, false>(c, c->wb, nullptr, nullptr, c->ru, nullptr);
+        if ((rc = col<CM_IZ_U>(c, self(c), 1, roles(B_W0, B_NONE, B_WB, B_NONE)))) return rc;
+        if ((rc = col<CM_Y_INV1>(c, self(c), 1, roles(B_WB, B_NONE, B_WB, B_NONE)))) return rc;
+        return row<RM_C2R, false>(c, self(c), 1, roles(B_WB, B_NONE, B_NONE, B_NONE, B_NONE, B_NONE,
+                                                       B_NONE, B_RU));
     }
 
     static int fixup(bfg_ctx* c) {
-        int rc = symmetrize(c, c->w0);
+        int rc = symmetrize(c, self(c), 1, B_W0);
         if (rc) return rc;
         const size_t npts = (size_t)N * N * c->nxv;
         Prof pr(c, K_KSPACE);
@@ -301,20 +312,23 @@ struct Engine {
     // unnormalised C2R of wb (state layout) into ru; uses wa
     static int ift_wb(bfg_ctx* c) {
         int rc;
-        if ((rc = col<CM_IZ_PLAIN>(c, 0.0, c->wb, nullptr, c->wa, nullptr))) return rc;
-        if ((rc = col<CM_Y_INV1>(c, 0.0, c->wa, nullptr, c->wa, nullptr))) return rc;
-        return row<RM_C2R, false>(c, c->wa, nullptr, nullptr, c->ru, nullptr);
+        if ((rc = col<CM_IZ_PLAIN>(c, self(c), 1, roles(B_WB, B_NONE, B_WA, B_NONE)))) return rc;
+        if ((rc = col<CM_Y_INV1>(c, self(c), 1, roles(B_WA, B_NONE, B_WA, B_NONE)))) return rc;
+        return row<RM_C2R, false>(c, self(c), 1, roles(B_WA, B_NONE, B_NONE, B_NONE, B_NONE, B_NONE,
+                                                       B_NONE, B_RU));
     }
     // unnormalised R2C of ru into wb (state layout); uses wa
     static int dft_ru(bfg_ctx* c) {
         int rc;
-        if ((rc = row<RM_R2C, false>(c, nullptr, nullptr, c->wa, nullptr, c->ru))) return rc;
-        if ((rc = col<CM_Y_FWD1>(c, 0.0, c->wa, nullptr, c->wa, nullptr))) return rc;
-        return col<CM_FZ_PLAIN>(c, 0.0, c->wa, nullptr, c->wb, nullptr);
+        if ((rc = row<RM_R2C, false>(c, self(c), 1, roles(B_NONE, B_NONE, B_WA, B_NONE, B_NONE,
+                                                          B_NONE, B_NONE, B_NONE, B_RU))))
+            return rc;
+        if ((rc = col<CM_Y_FWD1>(c, self(c), 1, roles(B_WA, B_NONE, B_WA, B_NONE)))) return rc;
+        return col<CM_FZ_PLAIN>(c, self(c), 1, roles(B_WA, B_NONE, B_WB, B_NONE));
     }
 
-    static int stats(bfg_ctx* c, const void* cfield, double max_est, int nbins, double* spec,
-                     double* mom, int64_t* hist);
+    static int stats(bfg_ctx* c, int cfield, double max_est, int nbins, double* spec, double* mom,
+                     int64_t* hist);
 };
 
 #include "stats_engine.inl"
@@ -372,8 +386,7 @@ struct OpDft {
 };
 template <typename T, int N>
 struct OpStats {
-    static int run(bfg_ctx* c, const void* f, double me, int nb, double* s, double* m,
-                   int64_t* h) {
+    static int run(bfg_ctx* c, int f, double me, int nb, double* s, double* m, int64_t* h) {
         return Engine<T, N>::stats(c, f, me, nb, s, m, h);
     }
 };
@@ -487,6 +500,34 @@ static int ensure_factors(bfg_ctx* c, double dt) {
     return 0;
 }
 
+// (re)upload this context's Member<T> when parameters or buffers changed
+template <typename T>
+static int sync_member_t(bfg_ctx* c, double dt) {
+    Member<T> m;
+    memset(&m, 0, sizeof(m));
+    m.kp = kparams(c, dt);
+    m.buf[B_W0] = (cpx<T>*)c->w0;
+    m.buf[B_V1] = (cpx<T>*)c->v1;
+    m.buf[B_V2] = (cpx<T>*)c->v2;
+    m.buf[B_WA] = (cpx<T>*)c->wa;
+    m.buf[B_WB] = (cpx<T>*)c->wb;
+    m.ru = (T*)c->ru;
+    m.filt = (const T*)c->filt;
+    m.fac = (const T*)c->fac;
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(&m);
+    if (c->dmember && c->hmember.size() == sizeof(m) && memcmp(c->hmember.data(), b, sizeof(m)) == 0)
+        return 0;
+    if (!c->dmember) CU(cudaMalloc(&c->dmember, sizeof(m)));
+    CU(cudaMemcpyAsync(c->dmember, b, sizeof(m), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    c->hmember.assign(b, b + sizeof(m));
+    return 0;
+}
+static int sync_member(bfg_ctx* c, double dt) {
+    if (std::isnan(dt)) dt = 0.0;
+    return c->real_bytes == 4 ? sync_member_t<float>(c, dt) : sync_member_t<double>(c, dt);
+}
+
 static int ensure_ru(bfg_ctx* c) {
     if (c->ru) return 0;
     const size_t bytes = (size_t)c->n * c->n * c->n * 3 * c->real_bytes;
@@ -588,12 +629,13 @@ static int tracer_loop(bfg_pctx* p, double dt) {
 
 template <typename T, int N>
 int OpStep<T, N>::run(bfg_ctx* c, double dt, bfg_pctx* p) {
+    using E = Engine<T, N>;
     int rc;
-    if ((rc = Engine<T, N>::stage(c, 0, dt, p != nullptr))) return rc;
+    if ((rc = E::stage(c, E::self(c), 1, 0, p != nullptr))) return rc;
     if (p && (rc = tracer_loop(p, dt))) return rc;
-    if ((rc = Engine<T, N>::stage(c, 1, dt, false))) return rc;
-    if ((rc = Engine<T, N>::stage(c, 2, dt, false))) return rc;
-    return Engine<T, N>::finish_step(c);
+    if ((rc = E::stage(c, E::self(c), 1, 1, false))) return rc;
+    if ((rc = E::stage(c, E::self(c), 1, 2, false))) return rc;
+    return E::finish_step(c, E::self(c), 1);
 }
 
 // ================================================================ ABI ==
@@ -607,7 +649,8 @@ void bfg_ctx_destroy(bfg_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* bufs[] = {c->w0, c->v1, c->v2, c->wa, c->wb, c->ru, c->tw, c->filt, c->fac, c->stats_ws};
+    void* bufs[] = {c->w0, c->v1, c->v2, c->wa, c->wb, c->ru, c->tw, c->filt, c->fac, c->stats_ws,
+                    c->dmember};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
@@ -766,7 +809,9 @@ int bfg_field_download(bfg_ctx* c, int field_id, void* host) {
 int bfg_read_checkpoint_fixup(bfg_ctx* c) {
     if (!c) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
-    int rc = dispatch<OpFixup>(c);
+    int rc = sync_member(c, c->fac_dt);
+    if (rc) return rc;
+    rc = dispatch<OpFixup>(c);
     if (rc) return rc;
     CU(cudaStreamSynchronize(c->stream));
     return 0;
@@ -779,6 +824,7 @@ int bfg_nsveparticles_step(bfg_ctx* c, bfg_pctx* p, double dt, int nsteps) {
     int rc = ensure_factors(c, dt);
     if (rc) return rc;
     if (p && (rc = ensure_ru(c))) return rc;
+    if ((rc = sync_member(c, dt))) return rc;
     CU(cudaEventRecord(c->ev0, c->stream));
     for (int s = 0; s < nsteps; ++s) {
         if ((rc = dispatch<OpStep>(c, dt, p))) return rc;
@@ -793,7 +839,9 @@ int bfg_step(bfg_ctx* c, double dt, int nsteps) { return bfg_nsveparticles_step(
 int bfg_compute_velocity(bfg_ctx* c) {
     if (!c) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
-    int rc = dispatch<OpVelocity>(c);
+    int rc = sync_member(c, c->fac_dt);
+    if (rc) return rc;
+    rc = dispatch<OpVelocity>(c);
     if (rc) return rc;
     CU(cudaStreamSynchronize(c->stream));
     return 0;
@@ -804,6 +852,7 @@ int bfg_velocity_rspace(bfg_ctx* c) {
     CU(cudaSetDevice(c->device));
     int rc = ensure_ru(c);
     if (rc) return rc;
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
     rc = dispatch<OpVelocityR>(c);
     if (rc) return rc;
     CU(cudaStreamSynchronize(c->stream));
@@ -816,6 +865,7 @@ int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
     int rc = ensure_ru(c);
     if (rc) return rc;
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
     CU(cudaMemcpy2DAsync(c->wb, c->nxp * 3 * cb, din, c->nxv * 3 * cb, c->nxv * 3 * cb, N * N,
                          cudaMemcpyDeviceToDevice, c->stream));
     if ((rc = dispatch<OpIft>(c))) return rc;
@@ -832,6 +882,7 @@ int bfg_dft(bfg_ctx* c, const void* din, void* dout) {
     int rc = ensure_ru(c);
     if (rc) return rc;
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
     CU(cudaMemcpy2DAsync(c->ru, N * 3 * rb, din, (N + 2) * 3 * rb, N * 3 * rb, N * N,
                          cudaMemcpyDeviceToDevice, c->stream));
     if ((rc = dispatch<OpDft>(c))) return rc;
@@ -898,11 +949,12 @@ int bfg_stats(bfg_ctx* c, double max_velocity_estimate, double max_vorticity_est
     int rc = ensure_ru(c);
     if (rc) return rc;
     // vorticity: state itself; velocity: compute_velocity(cvorticity)
-    if ((rc = dispatch<OpStats>(c, (const void*)c->w0, max_vorticity_estimate / std::sqrt(3.0),
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
+    if ((rc = dispatch<OpStats>(c, (int)B_W0, max_vorticity_estimate / std::sqrt(3.0),
                                 nbins, spec_vort, mom_vort, hist_vort)))
         return rc;
     if ((rc = dispatch<OpVelocity>(c))) return rc;
-    if ((rc = dispatch<OpStats>(c, (const void*)c->wa, max_velocity_estimate / std::sqrt(3.0),
+    if ((rc = dispatch<OpStats>(c, (int)B_WA, max_velocity_estimate / std::sqrt(3.0),
                                 nbins, spec_vel, mom_vel, hist_vel)))
         return rc;
     return 0;

@@ -38,6 +38,40 @@ struct KParams {
     double dt;
 };
 
+// One DNS instance as the kernels see it: parameters, its five complex
+// buffers (0 w0 = state, 1 v1, 2 v2, 3 wa, 4 wb), real velocity and tables.
+// A launch covers an array of members of the same N.
+template <typename T>
+struct Member {
+    KParams kp;
+    cpx<T>* buf[5];
+    T* ru;
+    const T* filt;
+    const T* fac;
+};
+enum BufIdx { B_W0 = 0, B_V1 = 1, B_V2 = 2, B_WA = 3, B_WB = 4, B_RU = 5, B_NONE = -1 };
+// which buffers play which part in one launch (B_* indices; rout / rin may
+// also name a complex buffer used as real scratch)
+struct Roles {
+    int in0, in1, out0, out1, v0, vp, fsrc, rout, rin;
+};
+__host__ __device__ inline Roles roles(int in0, int in1, int out0, int out1, int v0 = B_NONE,
+                                       int vp = B_NONE, int fsrc = B_NONE, int rout = B_NONE,
+                                       int rin = B_NONE) {
+    Roles r;
+    r.in0 = in0; r.in1 = in1; r.out0 = out0; r.out1 = out1;
+    r.v0 = v0; r.vp = vp; r.fsrc = fsrc; r.rout = rout; r.rin = rin;
+    return r;
+}
+template <typename T>
+__device__ __forceinline__ cpx<T>* mbuf(const Member<T>& m, int i) {
+    return i >= 0 && i < 5 ? m.buf[i] : nullptr;
+}
+template <typename T>
+__device__ __forceinline__ T* mreal(const Member<T>& m, int i) {
+    return i == B_RU ? m.ru : (i >= 0 && i < 5 ? reinterpret_cast<T*>(m.buf[i]) : nullptr);
+}
+
 enum ColMode {
     CM_IZ_VEL = 0,    // S -> (u^, w^) in W
     CM_IZ_PLAIN = 1,  // S -> W (inverse over kz)
@@ -271,11 +305,8 @@ __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
 
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(COL_THREADS, 1)
-col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restrict__ in1,
-         cpx<T>* out0, cpx<T>* out1, const cpx<T>* __restrict__ rk_v0,
-         const cpx<T>* __restrict__ rk_vp, const cpx<T>* __restrict__ fsrc,
-         const T* __restrict__ filt, const T* __restrict__ fac,
-         const cpx<T>* __restrict__ tw_g, int ntx, int ntiles) {
+col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
+         int ntx, int tiles_per, int ntiles) {
     constexpr int NB = col_nb(MODE);
     constexpr int TKX = col_tkx<T, N, MODE>();
     constexpr int W = 3 * TKX;                     // complex per row per buffer
@@ -292,24 +323,32 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
     cpx<T>* rkt = bufs + 2 * TILE;        // RK operand tile [arr][l][W] (FZ passes)
     cpx<T>* tw = rkt + NRK * N * W;
 
+    constexpr int NXV = N / 2 + 1;
+    constexpr size_t nxp3 = (size_t)(N / 2 + 4) * 3;
     const int tid = threadIdx.x;
-    const size_t nxp3 = (size_t)kp.nxp * 3;
     for (int i = tid; i < N; i += COL_THREADS) tw[i] = tw_g[i];
 
+    // tile t: member t / tiles_per, then (a, kx-tile) with the kx-tile fastest
     int t = blockIdx.x;
     if (t < ntiles) {
-        const int kx0 = (t % ntx) * TKX;
-        col_issue_load<T, N, MODE>(bufs, in0, in1, t / ntx, kx0, min(TKX, kp.nxv - kx0), nxp3, tid);
+        const int m = t / tiles_per, tl = t - m * tiles_per;
+        const int kx0 = (tl % ntx) * TKX;
+        col_issue_load<T, N, MODE>(bufs, mbuf(mem[m], rl.in0), mbuf(mem[m], rl.in1), tl / ntx, kx0,
+                                   min(TKX, NXV - kx0), nxp3, tid);
     }
     cp_async_commit();
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
         cpx<T>* tile = bufs + (it & 1) * TILE;
+        const int m = t / tiles_per, tl = t - m * tiles_per;
+        const Member<T>& mb = mem[m];
         if constexpr (NRK > 0) {
             // RK operands of this tile: rows S[ky=a][kz=l], streamed while the
             // tile is transformed (the epilogue of the previous tile is done)
-            const int a = t / ntx;
-            const int kx0 = (t % ntx) * TKX;
-            const int nvalid = (3 * min(TKX, kp.nxv - kx0) + VPE - 1) / VPE;
+            const int a = tl / ntx;
+            const int kx0 = (tl % ntx) * TKX;
+            const cpx<T>* rk_v0 = mbuf(mb, rl.v0);
+            const cpx<T>* rk_vp = mbuf(mb, rl.vp);
+            const int nvalid = (3 * min(TKX, NXV - kx0) + VPE - 1) / VPE;
             for (int e = tid; e < N * NRK * WV; e += COL_THREADS) {
                 const int v = e % WV;
                 const int r = e / WV;
@@ -325,18 +364,21 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
         {
             const int tn = t + gridDim.x;
             if (tn < ntiles) {
-                const int kx0n = (tn % ntx) * TKX;
-                col_issue_load<T, N, MODE>(bufs + ((it + 1) & 1) * TILE, in0, in1, tn / ntx, kx0n,
-                                           min(TKX, kp.nxv - kx0n), nxp3, tid);
+                const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
+                const int kx0n = (tln % ntx) * TKX;
+                col_issue_load<T, N, MODE>(bufs + ((it + 1) & 1) * TILE, mbuf(mem[mn], rl.in0),
+                                           mbuf(mem[mn], rl.in1), tln / ntx, kx0n,
+                                           min(TKX, NXV - kx0n), nxp3, tid);
             }
             cp_async_commit();
         }
         if constexpr (NRK > 0) cp_async_wait<2>();
         else cp_async_wait<1>();
         __syncthreads();
-        const int a = t / ntx;
-        const int kx0 = (t % ntx) * TKX;
-        const int ncol = min(TKX, kp.nxv - kx0);
+        const int a = tl / ntx;
+        const int kx0 = (tl % ntx) * TKX;
+        const int ncol = min(TKX, NXV - kx0);
+        const KParams& kp = mb.kp;
 
         // ---- prologue: u^ = i k x w^ / k^2 for 0 < k^2 <= kM^2 -----------
         if constexpr (MODE == CM_IZ_VEL || MODE == CM_IZ_U) {
@@ -380,11 +422,11 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
                 const int col = e % TKX;
                 const int l = e / TKX;
                 if (col >= ncol) continue;
-                const size_t pt = ((size_t)a * N + l) * kp.nxp + kx0 + col;  // S[ky=a][kz=l][kx]
+                const size_t pt = ((size_t)a * N + l) * (N / 2 + 4) + kx0 + col;  // S[ky=a][kz=l][kx]
                 const cpx<T>* v0 = &rkt[l * W + col * 3];
                 const cpx<T>* vp = &rkt[((NRK - 1) * N + l) * W + col * 3];
-                fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, ky, v0, vp, pt, filt,
-                                     fac, fsrc, out0);
+                fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, ky, v0, vp, pt, mb.filt,
+                                     mb.fac, mbuf(mb, rl.fsrc), mbuf(mb, rl.out0));
             }
         } else {
             dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, COL_THREADS);
@@ -403,7 +445,7 @@ col_pass(const KParams kp, const cpx<T>* __restrict__ in0, const cpx<T>* __restr
                 dft<T, INV, R>(v);
                 const int bufi = pp / W, q = pp % W;
                 if (q >= nval) continue;
-                cpx<T>* dst = ((bufi == 0) ? out0 : out1) + (size_t)kx0 * 3 + q;
+                cpx<T>* dst = mbuf(mb, (bufi == 0) ? rl.out0 : rl.out1) + (size_t)kx0 * 3 + q;
                 const int f0 = dif_frequency<N>(bb * R);
 #pragma unroll
                 for (int m = 0; m < R; ++m)
@@ -541,9 +583,8 @@ __device__ __forceinline__ void row_issue_load(cpx<T>* stage, const cpx<T>* wu, 
 
 template <typename T, int N, int MODE, bool WRITE_RU>
 __global__ void __launch_bounds__(ROW_THREADS, 1)
-row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restrict__ ww,
-         cpx<T>* wout, T* __restrict__ rout, const T* __restrict__ rin,
-         const cpx<T>* __restrict__ tw_g, int ntiles) {
+row_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
+         int tiles_per, int ntiles) {
     constexpr int M = N / 2;
     constexpr int ROWS = row_rows<T, N, MODE>();
     constexpr int RL = row_rl<N>();
@@ -568,21 +609,32 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
         for (int i = tid; i < ROWS * RL; i += ROW_THREADS) outr[i] = zero_c<T>();
     }
 
+    // tile t: member t / tiles_per, then ROWS consecutive rows
     int t = blockIdx.x;
-    if (t < ntiles) row_issue_load<T, N, MODE>(stage0, wu, ww, rin, (size_t)t * ROWS, tid);
+    if (t < ntiles) {
+        const int m = t / tiles_per, tl = t - m * tiles_per;
+        row_issue_load<T, N, MODE>(stage0, mbuf(mem[m], rl.in0), mbuf(mem[m], rl.in1),
+                                   mreal(mem[m], rl.rin), (size_t)tl * ROWS, tid);
+    }
     cp_async_commit();
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
         cpx<T>* st = stage0 + (it & 1) * STAGE;
         {
             const int tn = t + gridDim.x;
-            if (tn < ntiles)
-                row_issue_load<T, N, MODE>(stage0 + ((it + 1) & 1) * STAGE, wu, ww, rin,
-                                           (size_t)tn * ROWS, tid);
+            if (tn < ntiles) {
+                const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
+                row_issue_load<T, N, MODE>(stage0 + ((it + 1) & 1) * STAGE, mbuf(mem[mn], rl.in0),
+                                           mbuf(mem[mn], rl.in1), mreal(mem[mn], rl.rin),
+                                           (size_t)tln * ROWS, tid);
+            }
             cp_async_commit();
         }
         cp_async_wait<1>();
         __syncthreads();
-        const size_t row0 = (size_t)t * ROWS;
+        const int m = t / tiles_per, tl = t - m * tiles_per;
+        const size_t row0 = (size_t)tl * ROWS;
+        T* rout = mreal(mem[m], rl.rout);
+        cpx<T>* wout = mbuf(mem[m], rl.out0);
 
         if constexpr (MODE == RM_R2C) {
             // real rows -> digit-reversed complex pencils z_c[n] = (x[2n][c], x[2n+1][c])
@@ -669,9 +721,11 @@ row_pass(const KParams kp, const cpx<T>* __restrict__ wu, const cpx<T>* __restri
 // field::symmetrize on the kx = 0 plane of a state-layout buffer
 // (field.cpp:903-978).  One thread per (ky, kz) of the plane.
 template <typename T, int N>
-__global__ void symmetrize_kernel(cpx<T>* s, int nxp) {
+__global__ void symmetrize_kernel(const Member<T>* __restrict__ mem, int bufi) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= N * N) return;
+    cpx<T>* s = mem[blockIdx.y].buf[bufi];
+    const int nxp = N / 2 + 4;
     const int ky = e / N, kz = e % N;
     const size_t P = (size_t)nxp;
     auto at = [&](int y, int z) -> cpx<T>* { return s + ((size_t)y * N + z) * P * 3; };

@@ -5,7 +5,7 @@
 // Included by bfps_b200.cu after the Engine definition.
 
 template <typename T, int N>
-int Engine<T, N>::stats(bfg_ctx* c, const void* cfield, double max_est, int nbins, double* spec,
+int Engine<T, N>::stats(bfg_ctx* c, int cfield, double max_est, int nbins, double* spec,
                         double* mom, int64_t* hist) {
     const size_t spec_n = (size_t)c->nshells * 9;
     const size_t need = spec_n * 8 + (size_t)STATS_BLOCKS * NQ * 8 + NQ * 8 +
@@ -25,14 +25,17 @@ int Engine<T, N>::stats(bfg_ctx* c, const void* cfield, double max_est, int nbin
     CU(cudaMemsetAsync(d_hist, 0, (size_t)nbins * 4 * 8, c->stream));
     const KParams kp = kparams(c, 0.0);
     Prof pr0(c, K_STATS);
+    const void* cptr = cfield == B_W0 ? c->w0 : c->wa;
     spectrum_kernel<T, N><<<STATS_BLOCKS, 256, spec_n * 8, c->stream>>>(
-        kp, (const C*)cfield, c->nshells, c->dk, d_spec);
+        kp, (const C*)cptr, c->nshells, c->dk, d_spec);
     int rc = after_launch(c, "spectrum");
     if (rc) return rc;
     // real-space field into v2 (as [z][y][x][3] reals)
-    if ((rc = col<CM_IZ_PLAIN>(c, 0.0, cfield, nullptr, c->wb, nullptr))) return rc;
-    if ((rc = col<CM_Y_INV1>(c, 0.0, c->wb, nullptr, c->wb, nullptr))) return rc;
-    if ((rc = row<RM_C2R, false>(c, c->wb, nullptr, nullptr, c->v2, nullptr))) return rc;
+    if ((rc = col<CM_IZ_PLAIN>(c, self(c), 1, roles(cfield, B_NONE, B_WB, B_NONE)))) return rc;
+    if ((rc = col<CM_Y_INV1>(c, self(c), 1, roles(B_WB, B_NONE, B_WB, B_NONE)))) return rc;
+    if ((rc = row<RM_C2R, false>(c, self(c), 1, roles(B_WB, B_NONE, B_NONE, B_NONE, B_NONE,
+                                                     B_NONE, B_NONE, B_V2))))
+        return rc;
     const double me3 = max_est * std::sqrt(3.0);
     const size_t npts = (size_t)N * N * N;
     CU(ensure_smem(moments_kernel<T>, (size_t)nbins * 4 * 4, c->device));
