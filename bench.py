@@ -43,6 +43,14 @@ WORKLOADS = {
     # 32^3 FP64, 1024 tracers, 6-point Lagrange, AB2, 2/3 dealiasing
     "C1": dict(n=32, precision="double", nu=0.1, dt=0.01, k0=3.0, ntracers=1024,
                neighbours=2, smoothness=0, nsteps_ab=2, dealias=0),
+    # batched ensemble: 40 x 32^3, 16 x 64^3, 8 x 128^3, FP32, 1e4 Lagrange-6 tracers
+    # each, AB4, dt from CFL 0.5, 500-step solves
+    "C4": dict(kind="ensemble", sizes=[32] * 40 + [64] * 16 + [128] * 8, precision="single",
+               nu_range=(0.005, 0.05), ntracers=10_000, neighbours=2, smoothness=0, nsteps_ab=4,
+               solve_steps=500),
+    # serving: Poisson arrivals (20/s), N in {64: 0.6, 128: 0.3, 256: 0.1}, FP32,
+    # 100..1000 steps, 0..1e5 cubic-spline tracers, HBM budget 150 GB
+    "C5": dict(kind="serving", rate=20.0, requests=60, budget=150e9, precision="single"),
 }
 FORCING = dict(forcing_type="linear", fk0=1.5, fk1=3.0, famplitude=0.5)
 KIND_NAMES = ["IZ", "IY", "X", "FY", "FZ", "kspace", "tracers", "stats"]
@@ -327,6 +335,199 @@ def run_ours(args, cfg):
         print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------ batched / served ---
+def _ensemble_requests(cfg):
+    from bfps_b200 import serve
+    rng = np.random.default_rng(1000)
+    reqs = []
+    for i, n in enumerate(cfg["sizes"]):
+        nu = float(np.exp(rng.uniform(np.log(cfg["nu_range"][0]), np.log(cfg["nu_range"][1]))))
+        r = serve.Request(rid=i, n=n, nu=nu, steps=cfg["solve_steps"], ntracers=cfg["ntracers"],
+                          arrival=0.0, seed=i, precision=cfg["precision"],
+                          neighbours=cfg["neighbours"], smoothness=cfg["smoothness"],
+                          nsteps_ab=cfg["nsteps_ab"])
+        serve.prepare(r)
+        reqs.append(r)
+    return reqs
+
+
+def _member(r, device=0):
+    from bfps_b200.solver import vorticity_equation, particles_system
+    fs = vorticity_equation(r.n, precision=r.precision, device=device)
+    fs.nu = r.nu
+    fs.forcing_type = FORCING["forcing_type"]
+    fs.fk0, fs.fk1, fs.famplitude = FORCING["fk0"], FORCING["fk1"], FORCING["famplitude"]
+    fs.set_cvorticity(r.w0)
+    ps = particles_system(fs, r.pos, r.neighbours, r.smoothness, r.nsteps_ab) if r.ntracers else None
+    return fs, ps
+
+
+def ensemble_bytes(reqs):
+    """105 U per instance step + n*24*(k+2) + 6 N^3 P per instance (tracers)."""
+    tot = 0
+    for r in reqs:
+        P = 4 if r.precision == "single" else 8
+        U = r.n * r.n * (r.n + 2) * P
+        tot += 105 * U + r.ntracers * 24 * (r.nsteps_ab + 2) + 6 * r.n ** 3 * P
+    return tot
+
+
+def run_ensemble(args, cfg):
+    import torch
+    from bfps_b200.solver import ensemble, NSVEparticles_step
+    world, rank, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    reqs = _ensemble_requests(cfg)
+    members = [_member(r, local) for r in reqs]
+    ens = ensemble(local)
+    for (fs, ps), r in zip(members, reqs):
+        ens.add(fs, r.dt, ps)
+    ens.step(args.warmup)
+    ens.last_ms()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    ens.step(args.steps)
+    ms = ens.last_ms()
+    barrier(pg)
+    clk = clocks.stop()
+    ms = allmax(pg, ms)
+    ms_step = ms / args.steps
+    nsolve = len(reqs)
+    solves_s = world * nsolve / (cfg["solve_steps"] * ms_step / 1e3)
+    # the plain path one instance at a time: every member stepped alone with
+    # the single-instance entry point (same kernels, one launch per pass each)
+    seq_ms = 0.0
+    timed = {}
+    for (fs, ps), r in zip(members, reqs):
+        key = r.n
+        if key not in timed:
+            NSVEparticles_step(fs, ps, r.dt, 2)
+            fs.last_step_ms()
+            NSVEparticles_step(fs, ps, r.dt, max(3, args.steps // 2))
+            timed[key] = fs.last_step_ms() / max(3, args.steps // 2)
+        seq_ms += timed[key]
+    seq_solves_s = world * nsolve / (cfg["solve_steps"] * seq_ms / 1e3)
+    # end to end: every step the states go host -> device -> host
+    from bfps_b200 import _lib
+    L = _lib.lib()
+    host = []
+    for (fs, ps), r in zip(members, reqs):
+        w = torch.empty(int(np.prod(fs.cshape)), dtype=torch.complex64, pin_memory=True)
+        w = w.numpy().reshape(fs.cshape)
+        w[...] = fs.get_cvorticity()
+        host.append(w)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for (fs, ps), w in zip(members, host):
+            L.bfg_field_upload(fs.handle, _lib.FIELD_VORTICITY, w.ctypes.data)
+        ens.step(1)
+        ens.last_ms()
+        for (fs, ps), w in zip(members, host):
+            L.bfg_field_download(fs.handle, _lib.FIELD_VORTICITY, w.ctypes.data)
+    e2e_s = allmax(pg, time.perf_counter() - t0)
+    nbytes = sum(w.nbytes for w in host)
+    e2e_solves = world * nsolve / (cfg["solve_steps"] * e2e_s / e2e_steps)
+    peak, peak_kind = peaks()
+    step_bytes = ensemble_bytes(reqs)
+    ach = step_bytes / (ms_step / 1e3) / 1e9
+    out = {
+        "metric": "batched solves/s (mixed 32^3/64^3/128^3 ensemble)",
+        "value": round(solves_s, 4), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if cfg["precision"] == "single" else "f64",
+        "data": "synthetic (seeded fields per instance, uniform tracers)",
+        "config": {"workload": "C4: 64 instances (40x32^3, 16x64^3, 8x128^3) fp32, nu log-uniform "
+                               "[0.005, 0.05], CFL-0.5 dt, 1e4 Lagrange-6 tracers each, AB4, "
+                               "500-step solves",
+                   "instances": nsolve, "parallelism": "replicas x%d" % world,
+                   "l2": "ensemble state 2.4 GB > L2"},
+        "roofline": {"bound": "hbm", "kernel": "ensemble step (all passes)", "achieved": round(ach, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None},
+        "sequential": {"solves_s": round(seq_solves_s, 4), "ms_per_ensemble_step": round(seq_ms, 4),
+                       "speedup": round(solves_s / seq_solves_s, 3),
+                       "how": "each instance stepped alone with the single-instance entry point"},
+        "e2e": {"value": round(e2e_solves, 4), "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
+                "d2h_bytes_per_step": int(nbytes), "steps": e2e_steps},
+        "gpu_launches": None,
+        "clocks": clk,
+    }
+    ens.close()
+    for fs, ps in members:
+        if ps is not None:
+            ps.close()
+        fs.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_serving(args, cfg):
+    import torch
+    from bfps_b200 import serve
+    from bfps_b200.solver import NSVEparticles_step
+    world, rank, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    reqs = serve.poisson_stream(cfg["requests"], rate=cfg["rate"], seed=2000 + rank)
+    for r in reqs:
+        r.precision = cfg["precision"]
+        serve.prepare(r)
+    # warm-up: one small solve through the server (kernels, attributes)
+    w = serve.Request(rid=-1, n=64, nu=0.01, steps=3, ntracers=10, arrival=0.0, seed=99,
+                      precision=cfg["precision"])
+    serve.prepare(w)
+    srv = serve.Server(hbm_budget=cfg["budget"], device=local)
+    srv.run([w])
+    srv.done.clear()
+    barrier(pg)
+    t0 = time.perf_counter()
+    done = srv.run(reqs)
+    wall = time.perf_counter() - t0
+    srv.close()
+    ttc = np.array([r.finished - r.arrival for r in done])
+    span = max(r.finished for r in done) - min(r.arrival for r in done)
+    solves_s = len(done) / span
+    # the plain path one request at a time: per-size single-instance step time
+    step_ms = {}
+    for n in sorted({r.n for r in reqs}):
+        r0 = next(r for r in reqs if r.n == n)
+        fs, ps = _member(r0, local)
+        NSVEparticles_step(fs, ps, r0.dt, 2)
+        fs.last_step_ms()
+        NSVEparticles_step(fs, ps, r0.dt, 5)
+        step_ms[n] = fs.last_step_ms() / 5
+        if ps is not None:
+            ps.close()
+        fs.close()
+    seq_s = sum(r.steps * step_ms[r.n] / 1e3 for r in reqs)
+    seq_solves_s = len(reqs) / seq_s
+    out = {
+        "metric": "served solves/s, p50/p99 time-to-completion (Poisson stream)",
+        "value": round(solves_s * world, 4), "unit": "solves/s", "n_gpus": world,
+        "steps": None, "warmup": 1, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic request stream",
+        "config": {"workload": "C5: %d requests, Poisson 20/s, N in {64:0.6,128:0.3,256:0.1}, nu "
+                               "log-uniform [0.002,0.02], 100..1000 steps, 0..1e5 n2m2 tracers, "
+                               "HBM budget 150 GB" % len(reqs),
+                   "parallelism": "replicas x%d" % world},
+        "p50_s": round(float(np.percentile(ttc, 50)), 4),
+        "p99_s": round(float(np.percentile(ttc, 99)), 4),
+        "completed": len(done), "wall_s": round(wall, 3),
+        "sequential": {"solves_s": round(seq_solves_s, 4), "speedup": round(solves_s / seq_solves_s, 3),
+                       "how": "sum of steps x single-instance step time per size"},
+        "e2e": {"value": round(solves_s * world, 4), "unit": "solves/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "note": "wall clock from arrival to read-back of every request"},
+    }
+    if pg is not None:
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 # ------------------------------------------------------------------ CPU ---
 def _cpu_sample(cfg, tracer_fraction):
     """One bounded sample of the step on the host cores, with the CPU
@@ -426,6 +627,10 @@ def main():
     cfg = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, cfg)
+    elif cfg.get("kind") == "ensemble":
+        run_ensemble(args, cfg)
+    elif cfg.get("kind") == "serving":
+        run_serving(args, cfg)
     else:
         run_ours(args, cfg)
 

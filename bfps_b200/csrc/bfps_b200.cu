@@ -59,7 +59,10 @@ struct bfg_ctx {
     size_t stats_ws_bytes = 0;
     size_t field_bytes = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t tstream = nullptr;  // tracers (overlap stages 2-3 of the fluid step)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_ru = nullptr;     // real velocity of this step written
+    cudaEvent_t ev_tr = nullptr;     // tracers of this step done
     int64_t launches = 0;
     std::string err;
     // per-kernel profiling (bfg_profile)
@@ -131,6 +134,7 @@ enum Kind { K_IZ = 0, K_IY = 1, K_X = 2, K_FY = 3, K_FZ = 4, K_KSPACE = 5, K_TRA
 static void prof_flush(bfg_ctx* c) {
     if (!c->prof_used) return;
     cudaStreamSynchronize(c->stream);
+    if (c->tstream) cudaStreamSynchronize(c->tstream);
     for (size_t i = 0; i < c->prof_used; ++i) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]) == cudaSuccess) {
@@ -143,8 +147,9 @@ static void prof_flush(bfg_ctx* c) {
 
 struct Prof {
     bfg_ctx* c;
+    cudaStream_t st;
     long slot = -1;
-    Prof(bfg_ctx* c_, int kind) : c(c_) {
+    Prof(bfg_ctx* c_, int kind, cudaStream_t s_ = nullptr) : c(c_), st(s_ ? s_ : c_->stream) {
         if (!c->prof) return;
         if (c->prof_used >= 4096) prof_flush(c);
         if (c->prof_used == c->prof_kind.size()) {
@@ -157,10 +162,10 @@ struct Prof {
         }
         slot = (long)c->prof_used++;
         c->prof_kind[slot] = kind;
-        cudaEventRecord(c->prof_ev[2 * slot], c->stream);
+        cudaEventRecord(c->prof_ev[2 * slot], st);
     }
     ~Prof() {
-        if (slot >= 0) cudaEventRecord(c->prof_ev[2 * slot + 1], c->stream);
+        if (slot >= 0) cudaEventRecord(c->prof_ev[2 * slot + 1], st);
     }
 };
 
@@ -528,6 +533,13 @@ static int sync_member(bfg_ctx* c, double dt) {
     return c->real_bytes == 4 ? sync_member_t<float>(c, dt) : sync_member_t<double>(c, dt);
 }
 
+// order the context's main stream after the tracer work queued on the
+// second stream (anything that reads or rewrites tracers or ru)
+static int join_tracers(bfg_ctx* c) {
+    CU(cudaStreamWaitEvent(c->stream, c->ev_tr, 0));
+    return 0;
+}
+
 static int ensure_ru(bfg_ctx* c) {
     if (c->ru) return 0;
     const size_t bytes = (size_t)c->n * c->n * c->n * 3 * c->real_bytes;
@@ -541,19 +553,21 @@ static int ensure_ru(bfg_ctx* c) {
 
 // ----------------------------------------------------------- tracers --
 template <typename T, int NB, int MM>
-static int launch_tracers(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out) {
+static int launch_tracers(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out,
+                          cudaStream_t st) {
     const unsigned blocks = (unsigned)((p->n + TRACER_THREADS - 1) / TRACER_THREADS);
     if (blocks == 0) return 0;
-    Prof pr(c, K_TRACER);
-    tracer_kernel<T, NB, MM><<<blocks, TRACER_THREADS, 0, c->stream>>>(
+    Prof pr(c, K_TRACER, st);
+    tracer_kernel<T, NB, MM><<<blocks, TRACER_THREADS, 0, st>>>(
         pp, (const T*)c->ru, p->pos, p->hist, out);
     return after_launch(c, "tracer_kernel");
 }
 
 template <typename T>
-static int tracers_dispatch(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out) {
+static int tracers_dispatch(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out,
+                            cudaStream_t st) {
 #define BFG_TR(NBv, MMv) \
-    if (p->neighbours == NBv && p->smoothness == MMv) return launch_tracers<T, NBv, MMv>(c, pp, p, out);
+    if (p->neighbours == NBv && p->smoothness == MMv) return launch_tracers<T, NBv, MMv>(c, pp, p, out, st);
     BFG_TR(1, 0) BFG_TR(1, 1) BFG_TR(1, 2)
     BFG_TR(2, 0) BFG_TR(2, 1) BFG_TR(2, 2)
     BFG_TR(3, 0) BFG_TR(3, 1) BFG_TR(3, 2)
@@ -584,21 +598,22 @@ static PParams pparams(const bfg_pctx* p, double dt, int move) {
 
 // counting sort of the tracers by (z, y) cell row (tracer_keys / bucket_scan /
 // tracer_scatter); swaps the state arrays with their second copies
-static int tracer_sort(bfg_pctx* p) {
+static int tracer_sort(bfg_pctx* p, cudaStream_t st = nullptr) {
     bfg_ctx* c = p->ctx;
+    if (!st) st = c->stream;
     if (p->n == 0) return 0;
     const unsigned blocks = (unsigned)((p->n + 255) / 256);
     const int nb = c->n * c->n;
     PParams pp = pparams(p, 0.0, 0);
-    Prof pr(c, K_TRACER);
-    CU(cudaMemsetAsync(p->count, 0, (size_t)nb * sizeof(unsigned), c->stream));
-    tracer_keys<<<blocks, 256, 0, c->stream>>>(pp, p->pos, p->key, p->rank, p->count);
+    Prof pr(c, K_TRACER, st);
+    CU(cudaMemsetAsync(p->count, 0, (size_t)nb * sizeof(unsigned), st));
+    tracer_keys<<<blocks, 256, 0, st>>>(pp, p->pos, p->key, p->rank, p->count);
     int rc = after_launch(c, "tracer_keys");
     if (rc) return rc;
-    bucket_scan<<<1, 1024, 0, c->stream>>>(p->count, p->offset, nb);
+    bucket_scan<<<1, 1024, 0, st>>>(p->count, p->offset, nb);
     if ((rc = after_launch(c, "bucket_scan"))) return rc;
-    tracer_scatter<<<blocks, 256, 0, c->stream>>>(pp, p->key, p->rank, p->offset, p->pos, p->hist,
-                                                   p->corder, p->pos2, p->hist2, p->corder2);
+    tracer_scatter<<<blocks, 256, 0, st>>>(pp, p->key, p->rank, p->offset, p->pos, p->hist,
+                                            p->corder, p->pos2, p->hist2, p->corder2);
     if ((rc = after_launch(c, "tracer_scatter"))) return rc;
     std::swap(p->pos, p->pos2);
     std::swap(p->hist, p->hist2);
@@ -607,17 +622,18 @@ static int tracer_sort(bfg_pctx* p) {
     return 0;
 }
 
-static int tracer_loop(bfg_pctx* p, double dt) {
+static int tracer_loop(bfg_pctx* p, double dt, cudaStream_t st = nullptr) {
     bfg_ctx* c = p->ctx;
+    if (!st) st = c->stream;
     if (p->loops_since_sort >= p->resort_every) {
-        int rc = tracer_sort(p);
+        int rc = tracer_sort(p, st);
         if (rc) return rc;
     }
     if (p->step_idx > 6 && p->nsteps > 6)
         return fail(c, BFG_EINVAL, "Adams-Bashforth order above 6");
     PParams pp = pparams(p, dt, 1);
-    int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, nullptr)
-                                : tracers_dispatch<double>(c, pp, p, nullptr);
+    int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, nullptr, st)
+                                : tracers_dispatch<double>(c, pp, p, nullptr, st);
     if (rc) return rc;
     // inc_step_idx, shift_rhs_vectors
     p->step_idx += 1;
@@ -631,8 +647,16 @@ template <typename T, int N>
 int OpStep<T, N>::run(bfg_ctx* c, double dt, bfg_pctx* p) {
     using E = Engine<T, N>;
     int rc;
+    // the previous step's tracers read ru, which stage 1 rewrites
+    if (p) CU(cudaStreamWaitEvent(c->stream, c->ev_tr, 0));
     if ((rc = E::stage(c, E::self(c), 1, 0, p != nullptr))) return rc;
-    if (p && (rc = tracer_loop(p, dt))) return rc;
+    if (p) {
+        // tracers on u(t) (written by stage 1).  They run on the main stream:
+        // running them beside the persistent passes of stages 2-3 was slower,
+        // both sides losing L1/L2 to the other.
+        if ((rc = tracer_loop(p, dt, c->stream))) return rc;
+        CU(cudaEventRecord(c->ev_tr, c->stream));
+    }
     if ((rc = E::stage(c, E::self(c), 1, 1, false))) return rc;
     if ((rc = E::stage(c, E::self(c), 1, 2, false))) return rc;
     return E::finish_step(c, E::self(c), 1);
@@ -654,6 +678,10 @@ void bfg_ctx_destroy(bfg_ctx* c) {
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+    if (c->tstream) cudaStreamSynchronize(c->tstream);
+    if (c->ev_ru) cudaEventDestroy(c->ev_ru);
+    if (c->ev_tr) cudaEventDestroy(c->ev_tr);
+    if (c->tstream) cudaStreamDestroy(c->tstream);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -713,8 +741,12 @@ int bfg_ctx_create(bfg_ctx** out, int nx, int ny, int nz, double dkx, double dky
             cudaSuccess)
         return bail(BFG_ECUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(BFG_ECUDA);
+    if (cudaStreamCreateWithFlags(&c->tstream, cudaStreamNonBlocking) != cudaSuccess) return bail(BFG_ECUDA);
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
+    cudaEventCreateWithFlags(&c->ev_ru, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->ev_tr, cudaEventDisableTiming);
+    cudaEventRecord(c->ev_tr, c->tstream);
     const size_t cb = 2 * (size_t)real_bytes;  // bytes per complex
     c->field_bytes = (size_t)nx * nx * c->nxp * 3 * cb;
     void** bufs[] = {&c->w0, &c->v1, &c->v2, &c->wa, &c->wb};
@@ -763,6 +795,7 @@ int bfg_kspace_info(const bfg_ctx* c, double* kM, double* dk, int* nshells, doub
 static int field_copy(bfg_ctx* c, int field_id, void* host, bool upload) {
     if (!c || !host) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     const size_t cb = 2 * (size_t)c->real_bytes;
     const size_t N = c->n;
     if (field_id == BFG_FIELD_VORTICITY || field_id == BFG_FIELD_VELOCITY) {
@@ -830,6 +863,7 @@ int bfg_nsveparticles_step(bfg_ctx* c, bfg_pctx* p, double dt, int nsteps) {
         if ((rc = dispatch<OpStep>(c, dt, p))) return rc;
         c->iteration++;
     }
+    if (p) CU(cudaStreamWaitEvent(c->stream, c->ev_tr, 0));
     CU(cudaEventRecord(c->ev1, c->stream));
     return 0;
 }
@@ -850,6 +884,7 @@ int bfg_compute_velocity(bfg_ctx* c) {
 int bfg_velocity_rspace(bfg_ctx* c) {
     if (!c) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     int rc = ensure_ru(c);
     if (rc) return rc;
     if ((rc = sync_member(c, c->fac_dt))) return rc;
@@ -862,6 +897,7 @@ int bfg_velocity_rspace(bfg_ctx* c) {
 int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
     if (!c || !din || !dout) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     int rc = ensure_ru(c);
     if (rc) return rc;
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
@@ -879,6 +915,7 @@ int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
 int bfg_dft(bfg_ctx* c, const void* din, void* dout) {
     if (!c || !din || !dout) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     int rc = ensure_ru(c);
     if (rc) return rc;
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
@@ -1060,7 +1097,11 @@ int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, 
 
 void bfg_particles_destroy(bfg_pctx* p) {
     if (!p) return;
-    if (p->ctx) cudaSetDevice(p->ctx->device);
+    if (p->ctx) {
+        cudaSetDevice(p->ctx->device);
+        cudaStreamSynchronize(p->ctx->tstream);
+        cudaStreamSynchronize(p->ctx->stream);
+    }
     void* bufs[] = {p->pos, p->pos2, p->hist, p->hist2, p->corder, p->corder2,
                     p->sample, p->key, p->rank, p->count, p->offset};
     for (void* b : bufs)
@@ -1072,6 +1113,7 @@ int bfg_particles_complete_loop(bfg_pctx* p, double dt) {
     if (!p) return BFG_EINVAL;
     bfg_ctx* c = p->ctx;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     int rc = tracer_loop(p, dt);
     if (rc) return rc;
     CU(cudaStreamSynchronize(c->stream));
@@ -1082,9 +1124,10 @@ int bfg_particles_sample_velocity(bfg_pctx* p, double* out) {
     if (!p || !out) return BFG_EINVAL;
     bfg_ctx* c = p->ctx;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     PParams pp = pparams(p, 0.0, 0);
-    int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, p->sample)
-                                : tracers_dispatch<double>(c, pp, p, p->sample);
+    int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, p->sample, c->stream)
+                                : tracers_dispatch<double>(c, pp, p, p->sample, c->stream);
     if (rc) return rc;
     return fetch_index_order(p, p->sample, 3, out);
 }
@@ -1093,6 +1136,7 @@ int bfg_particles_download(bfg_pctx* p, double* pos, double* rhs, int64_t* idx) 
     if (!p) return BFG_EINVAL;
     bfg_ctx* c = p->ctx;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     const size_t n3 = (size_t)p->n * 3;
     int rc;
     if (pos && (rc = fetch_index_order(p, p->pos, 3, pos))) return rc;
@@ -1120,6 +1164,7 @@ int bfg_particles_upload(bfg_pctx* p, const double* pos, const double* rhs, int 
     if (!p || (p->n > 0 && !pos) || step_idx < 1) return BFG_EINVAL;
     bfg_ctx* c = p->ctx;
     CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
     const size_t n3 = (size_t)p->n * 3;
     p->head = 0;
     p->step_idx = step_idx;
@@ -1310,3 +1355,307 @@ extern "C" int bfg_rspace_stats_noalloc(const void* dev_field, int nx, int ny, i
     if (cudaGetLastError() != cudaSuccess) return BFG_ECUDA;
     return BFG_OK;
 }
+
+// ============================================================== ensembles ==
+// Many independent instances advanced together: members of equal grid size
+// form a group, and every pass of an RK stage is one persistent launch over
+// all members of a group (the tile index decodes to member, then tile).
+// The fluid launches of each stage are captured once into CUDA graphs and
+// replayed; each member's tracers follow stage 1, which produces its u(t).
+
+struct EnsGroup {
+    int n = 0;
+    std::vector<int> members;  // indices into bfg_ens::entries
+    void* dmem = nullptr;      // Member<T>[members.size()]
+    size_t cap = 0;
+    bfg_ctx launcher;          // stream / SM count / twiddles / errors for this group's launches
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // stage 1 (+ru), 2, 3 + symmetrize
+    bool any_tracers = false;
+};
+
+struct bfg_ens {
+    int device = 0;
+    int real_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_ru = nullptr;
+    struct Entry {
+        bfg_ctx* ctx;
+        bfg_pctx* tracers;
+        double dt;
+    };
+    std::vector<Entry> entries;
+    std::vector<EnsGroup*> groups;
+    bool dirty = true;
+    bool use_graphs = true;
+    std::string err;
+};
+
+static int ens_fail(bfg_ens* e, int code, const char* msg) {
+    if (e) e->err = msg;
+    return code;
+}
+
+static void ens_free_groups(bfg_ens* e) {
+    for (EnsGroup* g : e->groups) {
+        for (auto& ge : g->graph)
+            if (ge) cudaGraphExecDestroy(ge);
+        if (g->dmem) cudaFree(g->dmem);
+        delete g;
+    }
+    e->groups.clear();
+}
+
+template <typename T>
+static Member<T> member_of(bfg_ctx* c, double dt) {
+    Member<T> m;
+    memset(&m, 0, sizeof(m));
+    m.kp = kparams(c, dt);
+    m.buf[B_W0] = (cpx<T>*)c->w0;
+    m.buf[B_V1] = (cpx<T>*)c->v1;
+    m.buf[B_V2] = (cpx<T>*)c->v2;
+    m.buf[B_WA] = (cpx<T>*)c->wa;
+    m.buf[B_WB] = (cpx<T>*)c->wb;
+    m.ru = (T*)c->ru;
+    m.filt = (const T*)c->filt;
+    m.fac = (const T*)c->fac;
+    return m;
+}
+
+template <typename T, int N>
+struct EnsOps {
+    using E = Engine<T, N>;
+    static int stage(EnsGroup* g, int s) {
+        const Member<T>* mem = (const Member<T>*)g->dmem;
+        const int nm = (int)g->members.size();
+        int rc = E::stage(&g->launcher, mem, nm, s, s == 0 && g->any_tracers);
+        if (rc) return rc;
+        if (s == 2) rc = E::finish_step(&g->launcher, mem, nm);
+        return rc;
+    }
+};
+
+template <typename T>
+static int ens_group_stage(EnsGroup* g, int s) {
+    switch (g->n) {
+        case 16: return EnsOps<T, 16>::stage(g, s);
+        case 32: return EnsOps<T, 32>::stage(g, s);
+        case 64: return EnsOps<T, 64>::stage(g, s);
+        case 128: return EnsOps<T, 128>::stage(g, s);
+        case 256: return EnsOps<T, 256>::stage(g, s);
+        case 512: return EnsOps<T, 512>::stage(g, s);
+        case 1024: return EnsOps<T, 1024>::stage(g, s);
+    }
+    return BFG_EUNSUP;
+}
+
+static int ens_stage(bfg_ens* e, EnsGroup* g, int s) {
+    return e->real_bytes == 4 ? ens_group_stage<float>(g, s) : ens_group_stage<double>(g, s);
+}
+
+// (re)build groups, member arrays and graphs after membership changes
+static int ens_prepare(bfg_ens* e) {
+    if (!e->dirty) return 0;
+    cudaSetDevice(e->device);
+    ens_free_groups(e);
+    std::vector<int> sizes;
+    for (auto& en : e->entries)
+        if (std::find(sizes.begin(), sizes.end(), en.ctx->n) == sizes.end()) sizes.push_back(en.ctx->n);
+    std::sort(sizes.rbegin(), sizes.rend());  // large grids first
+    for (int n : sizes) {
+        EnsGroup* g = new EnsGroup();
+        g->n = n;
+        for (int i = 0; i < (int)e->entries.size(); ++i)
+            if (e->entries[i].ctx->n == n) g->members.push_back(i);
+        bfg_ctx* c0 = e->entries[g->members[0]].ctx;
+        g->launcher.n = n;
+        g->launcher.nxv = c0->nxv;
+        g->launcher.nxp = c0->nxp;
+        g->launcher.nsm = c0->nsm;
+        g->launcher.smem_optin = c0->smem_optin;
+        g->launcher.real_bytes = c0->real_bytes;
+        g->launcher.device = c0->device;
+        g->launcher.tw = c0->tw;
+        g->launcher.stream = e->stream;
+        for (int i : g->members) g->any_tracers = g->any_tracers || e->entries[i].tracers != nullptr;
+        // member descriptors
+        std::vector<unsigned char> host;
+        for (int i : g->members) {
+            auto& en = e->entries[i];
+            if (e->real_bytes == 4) {
+                Member<float> m = member_of<float>(en.ctx, en.dt);
+                host.insert(host.end(), (unsigned char*)&m, (unsigned char*)&m + sizeof(m));
+            } else {
+                Member<double> m = member_of<double>(en.ctx, en.dt);
+                host.insert(host.end(), (unsigned char*)&m, (unsigned char*)&m + sizeof(m));
+            }
+        }
+        e->groups.push_back(g);
+        if (cudaMalloc(&g->dmem, host.size()) != cudaSuccess) {
+            cudaGetLastError();
+            return ens_fail(e, BFG_ENOMEM, "cannot allocate member descriptors");
+        }
+        if (cudaMemcpy(g->dmem, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return ens_fail(e, BFG_ECUDA, "member descriptor upload failed");
+        g->cap = host.size();
+        if (e->use_graphs) {
+            for (int s = 0; s < 3; ++s) {
+                cudaGraph_t graph = nullptr;
+                if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+                    return ens_fail(e, BFG_ECUDA, "stream capture failed to start");
+                int rc = ens_stage(e, g, s);
+                cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+                if (rc || ce != cudaSuccess) {
+                    if (graph) cudaGraphDestroy(graph);
+                    return ens_fail(e, rc ? rc : BFG_ECUDA,
+                                    rc ? g->launcher.err.c_str() : "stream capture failed");
+                }
+                ce = cudaGraphInstantiate(&g->graph[s], graph, 0);
+                cudaGraphDestroy(graph);
+                if (ce != cudaSuccess) return ens_fail(e, BFG_ECUDA, "graph instantiation failed");
+            }
+        }
+    }
+    e->dirty = false;
+    return 0;
+}
+
+extern "C" {
+
+int bfg_ens_create(bfg_ens** out, int device) {
+    if (!out) return BFG_EINVAL;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return BFG_ECUDA;
+    }
+    bfg_ens* e = new bfg_ens();
+    e->device = device;
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete e;
+        return BFG_ECUDA;
+    }
+    cudaEventCreate(&e->ev0);
+    cudaEventCreate(&e->ev1);
+    cudaEventCreateWithFlags(&e->ev_ru, cudaEventDisableTiming);
+    *out = e;
+    return 0;
+}
+
+void bfg_ens_destroy(bfg_ens* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    for (auto& en : e->entries) cudaStreamSynchronize(en.ctx->tstream);
+    ens_free_groups(e);
+    cudaEventDestroy(e->ev0);
+    cudaEventDestroy(e->ev1);
+    cudaEventDestroy(e->ev_ru);
+    cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+const char* bfg_ens_last_error(const bfg_ens* e) { return e ? e->err.c_str() : "null ensemble"; }
+
+int bfg_ens_add(bfg_ens* e, bfg_ctx* c, bfg_pctx* p, double dt) {
+    if (!e || !c || !(dt > 0)) return BFG_EINVAL;
+    if (p && p->ctx != c) return ens_fail(e, BFG_EINVAL, "tracers belong to another context");
+    if (c->device != e->device) return ens_fail(e, BFG_EINVAL, "member on another device");
+    if (e->real_bytes && c->real_bytes != e->real_bytes)
+        return ens_fail(e, BFG_EINVAL, "members must share one precision");
+    for (auto& en : e->entries)
+        if (en.ctx == c) return ens_fail(e, BFG_EINVAL, "context already in the ensemble");
+    cudaSetDevice(e->device);
+    int rc = ensure_factors(c, dt);
+    if (rc) return ens_fail(e, rc, c->err.c_str());
+    if ((rc = ensure_ru(c))) return ens_fail(e, rc, c->err.c_str());
+    // the member's own streams are idle from here on; the ensemble orders
+    // itself after anything still queued there
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaStreamSynchronize(c->tstream) != cudaSuccess)
+        return ens_fail(e, BFG_ECUDA, "member stream synchronisation failed");
+    e->real_bytes = c->real_bytes;
+    e->entries.push_back({c, p, dt});
+    e->dirty = true;
+    return 0;
+}
+
+int bfg_ens_remove(bfg_ens* e, bfg_ctx* c) {
+    if (!e || !c) return BFG_EINVAL;
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+    for (size_t i = 0; i < e->entries.size(); ++i)
+        if (e->entries[i].ctx == c) {
+            cudaStreamSynchronize(c->tstream);
+            e->entries.erase(e->entries.begin() + i);
+            e->dirty = true;
+            if (e->entries.empty()) e->real_bytes = 0;
+            return 0;
+        }
+    return ens_fail(e, BFG_EINVAL, "context not in the ensemble");
+}
+
+int bfg_ens_count(const bfg_ens* e, int* members) {
+    if (!e || !members) return BFG_EINVAL;
+    *members = (int)e->entries.size();
+    return 0;
+}
+
+int bfg_ens_step(bfg_ens* e, int nsteps) {
+    if (!e || nsteps < 0) return BFG_EINVAL;
+    if (e->entries.empty()) return 0;
+    cudaSetDevice(e->device);
+    int rc = ens_prepare(e);
+    if (rc) return rc;
+    if (cudaEventRecord(e->ev0, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
+    for (int st = 0; st < nsteps; ++st) {
+        // the previous step's tracers read ru, which stage 1 rewrites
+        for (auto& en : e->entries)
+            if (en.tracers) cudaStreamWaitEvent(e->stream, en.ctx->ev_tr, 0);
+        for (EnsGroup* g : e->groups) {
+            rc = e->use_graphs ? (cudaGraphLaunch(g->graph[0], e->stream) == cudaSuccess ? 0 : BFG_ECUDA)
+                               : ens_stage(e, g, 0);
+            if (rc) return ens_fail(e, rc, "stage 1 launch failed");
+        }
+        if (cudaEventRecord(e->ev_ru, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
+        for (auto& en : e->entries) {
+            if (!en.tracers) continue;
+            bfg_ctx* c = en.ctx;
+            if ((rc = tracer_loop(en.tracers, en.dt, e->stream))) return ens_fail(e, rc, c->err.c_str());
+            if (cudaEventRecord(c->ev_tr, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
+        }
+        for (int s = 1; s < 3; ++s)
+            for (EnsGroup* g : e->groups) {
+                rc = e->use_graphs
+                         ? (cudaGraphLaunch(g->graph[s], e->stream) == cudaSuccess ? 0 : BFG_ECUDA)
+                         : ens_stage(e, g, s);
+                if (rc) return ens_fail(e, rc, "stage launch failed");
+            }
+        for (auto& en : e->entries) en.ctx->iteration++;
+    }
+    for (auto& en : e->entries)
+        if (en.tracers) cudaStreamWaitEvent(e->stream, en.ctx->ev_tr, 0);
+    if (cudaEventRecord(e->ev1, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
+    // members' own streams follow the ensemble's work
+    for (auto& en : e->entries) cudaStreamWaitEvent(en.ctx->stream, e->ev1, 0);
+    cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) return ens_fail(e, BFG_ECUDA, cudaGetErrorString(ce));
+    return 0;
+}
+
+int bfg_ens_last_ms(bfg_ens* e, double* ms) {
+    if (!e || !ms) return BFG_EINVAL;
+    cudaSetDevice(e->device);
+    if (cudaEventSynchronize(e->ev1) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event sync");
+    float f = 0;
+    if (cudaEventElapsedTime(&f, e->ev0, e->ev1) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "timing");
+    *ms = f;
+    return 0;
+}
+
+int bfg_ens_use_graphs(bfg_ens* e, int enable) {
+    if (!e) return BFG_EINVAL;
+    e->use_graphs = enable != 0;
+    e->dirty = true;
+    return 0;
+}
+
+}  // extern "C"

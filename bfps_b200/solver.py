@@ -243,3 +243,52 @@ def NSVEparticles_step(fs, ps, dt, nsteps=1):
     """NSVEparticles::step (NSVEparticles.cpp:33-41), nsteps times."""
     check(lib().bfg_nsveparticles_step(fs.handle, ps.handle if ps is not None else None,
                                        float(dt), int(nsteps)), fs.handle)
+
+
+class ensemble:
+    """Batched form: many contexts advanced together (bfg_ens_*).
+
+    Members of equal grid size share one launch per pass and RK stage; the
+    result of every member is the same as stepping it alone.
+    """
+
+    def __init__(self, device=0):
+        h = ctypes.c_void_p()
+        check(lib().bfg_ens_create(ctypes.byref(h), device))
+        self._h = h
+        self.members = []
+
+    def _check(self, rc):
+        if rc != 0:
+            raise _lib.BfgError(rc, lib().bfg_ens_last_error(self._h).decode())
+
+    def add(self, fs, dt, tracers=None):
+        self._check(lib().bfg_ens_add(self._h, fs.handle,
+                                      tracers.handle if tracers is not None else None, float(dt)))
+        self.members.append((fs, tracers, dt))
+
+    def remove(self, fs):
+        self._check(lib().bfg_ens_remove(self._h, fs.handle))
+        self.members = [m for m in self.members if m[0] is not fs]
+
+    def step(self, nsteps=1):
+        self._check(lib().bfg_ens_step(self._h, int(nsteps)))
+
+    def last_ms(self):
+        ms = ctypes.c_double()
+        self._check(lib().bfg_ens_last_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def use_graphs(self, enable):
+        self._check(lib().bfg_ens_use_graphs(self._h, int(bool(enable))))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bfg_ens_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -160,6 +160,32 @@ int bfg_particles_upload(bfg_pctx* p, const double* pos, const double* rhs, int 
 int bfg_particles_download(bfg_pctx* p, double* pos, double* rhs, int64_t* idx);
 int bfg_particles_info(const bfg_pctx* p, int64_t* n, int* nsteps, int* step_idx);
 
+/* ------------------------------------------------------ ensembles ---- */
+
+/* Batched form (no counterpart in the single-instance reference; each
+ * member's step is vorticity_equation::step / NSVEparticles::step): many
+ * independent contexts of any sizes, viscosities and seeds, advanced
+ * together.  Members of equal grid size share one persistent launch per
+ * pass and RK stage; the fluid launches are replayed from CUDA graphs;
+ * tracers advance after stage 1 of the step, as in NSVEparticles::step.
+ * Members keep
+ * their state and API; while in an ensemble they must be stepped only
+ * through it.  All members share one device and one precision. */
+typedef struct bfg_ens bfg_ens;
+int bfg_ens_create(bfg_ens** out, int device);
+void bfg_ens_destroy(bfg_ens* e);
+const char* bfg_ens_last_error(const bfg_ens* e);
+/* add a member with its fixed time step (and optional tracers) */
+int bfg_ens_add(bfg_ens* e, bfg_ctx* member, bfg_pctx* tracers_or_null, double dt);
+int bfg_ens_remove(bfg_ens* e, bfg_ctx* member);
+int bfg_ens_count(const bfg_ens* e, int* members);
+/* nsteps NSVEparticles steps of every member */
+int bfg_ens_step(bfg_ens* e, int nsteps);
+/* device time of the last bfg_ens_step call (synchronises) */
+int bfg_ens_last_ms(bfg_ens* e, double* ms);
+/* replay the fluid launches from CUDA graphs (default 1) or launch directly */
+int bfg_ens_use_graphs(bfg_ens* e, int enable);
+
 /* ------------------------------------------------------ measurement ---- */
 
 /* Synchronise the context's stream and return the device time of the last
