@@ -95,7 +95,7 @@ struct bfg_pctx {
     unsigned* rank = nullptr;
     unsigned* count = nullptr;
     unsigned* offset = nullptr;
-    int resort_every = 4;
+    int resort_every = 4;    // 0: never (grids below 256^3 keep u in L2 anyway)
     int loops_since_sort = 0;
     std::vector<int64_t> idx;       // global index of each tracer, creation order
     std::vector<int64_t> by_index;  // creation positions sorted by global index
@@ -247,7 +247,7 @@ struct Engine {
         CU(ensure_smem(kern, smem, c->device));
         const int tiles_per = N * N / ROWS;
         const int ntiles = tiles_per * nmem;
-        const int grid = std::min(ntiles, c->nsm);
+        const int grid = std::min(ntiles, c->nsm * ROW_CTAS);
         Prof pr(c, K_X);
         kern<<<grid, ROW_THREADS, smem, c->stream>>>(mem, rl, (const C*)c->tw, tiles_per, ntiles);
         return after_launch(c, "row_pass");
@@ -625,7 +625,7 @@ static int tracer_sort(bfg_pctx* p, cudaStream_t st = nullptr) {
 static int tracer_loop(bfg_pctx* p, double dt, cudaStream_t st = nullptr) {
     bfg_ctx* c = p->ctx;
     if (!st) st = c->stream;
-    if (p->loops_since_sort >= p->resort_every) {
+    if (p->resort_every > 0 && p->loops_since_sort >= p->resort_every) {
         int rc = tracer_sort(p, st);
         if (rc) return rc;
     }
@@ -1057,6 +1057,7 @@ int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, 
     p->nsteps = nsteps;
     p->step_idx = step_idx;
     p->head = 0;
+    p->resort_every = c->n >= 256 ? 4 : 0;
     const size_t n1 = (size_t)std::max<int64_t>(n, 1);
     const size_t nb = n1 * 3 * sizeof(double);
     const size_t nbk = (size_t)c->n * c->n * sizeof(unsigned);
@@ -1385,6 +1386,12 @@ struct bfg_ens {
     };
     std::vector<Entry> entries;
     std::vector<EnsGroup*> groups;
+    // tracer systems advanced by one batched launch (same interpolation, no
+    // re-sorting); the others use their own loop
+    std::vector<int> batched;   // entry indices
+    void* dsets = nullptr;      // TracerSet[batched.size()]
+    void* dstart = nullptr;     // int64[batched.size() + 1]
+    int64_t nbatched = 0;
     bool dirty = true;
     bool use_graphs = true;
     std::string err;
@@ -1395,7 +1402,35 @@ static int ens_fail(bfg_ens* e, int code, const char* msg) {
     return code;
 }
 
+template <typename T, int NB, int MM>
+static int ens_tracers_launch(bfg_ens* e) {
+    const unsigned blocks = (unsigned)((e->nbatched + TRACER_THREADS - 1) / TRACER_THREADS);
+    if (blocks == 0) return 0;
+    tracer_batch_kernel<T, NB, MM><<<blocks, TRACER_THREADS, 0, e->stream>>>(
+        (const TracerSet*)e->dsets, (const int64_t*)e->dstart, (int)e->batched.size());
+    tracer_sets_advance<<<((int)e->batched.size() + 127) / 128, 128, 0, e->stream>>>(
+        (TracerSet*)e->dsets, (int)e->batched.size());
+    return cudaGetLastError() == cudaSuccess ? 0 : BFG_ECUDA;
+}
+template <typename T>
+static int ens_tracers_dispatch(bfg_ens* e, int nb, int mm) {
+#define BFG_ETR(NBv, MMv) \
+    if (nb == NBv && mm == MMv) return ens_tracers_launch<T, NBv, MMv>(e);
+    BFG_ETR(1, 0) BFG_ETR(1, 1) BFG_ETR(1, 2)
+    BFG_ETR(2, 0) BFG_ETR(2, 1) BFG_ETR(2, 2)
+    BFG_ETR(3, 0) BFG_ETR(3, 1) BFG_ETR(3, 2)
+    BFG_ETR(4, 0) BFG_ETR(4, 1) BFG_ETR(4, 2)
+    BFG_ETR(5, 0) BFG_ETR(5, 1) BFG_ETR(5, 2)
+#undef BFG_ETR
+    return BFG_EUNSUP;
+}
+
 static void ens_free_groups(bfg_ens* e) {
+    if (e->dsets) cudaFree(e->dsets);
+    if (e->dstart) cudaFree(e->dstart);
+    e->dsets = e->dstart = nullptr;
+    e->batched.clear();
+    e->nbatched = 0;
     for (EnsGroup* g : e->groups) {
         for (auto& ge : g->graph)
             if (ge) cudaGraphExecDestroy(ge);
@@ -1515,6 +1550,42 @@ static int ens_prepare(bfg_ens* e) {
             }
         }
     }
+    // batched tracer sets: every member with tracers on a grid below 256^3
+    // whose interpolation matches the first such member
+    std::vector<TracerSet> sets;
+    std::vector<int64_t> start(1, 0);
+    for (int i = 0; i < (int)e->entries.size(); ++i) {
+        auto& en = e->entries[i];
+        bfg_pctx* p = en.tracers;
+        if (!p || p->resort_every != 0 || p->n == 0) continue;
+        if (!e->batched.empty()) {
+            bfg_pctx* p0 = e->entries[e->batched[0]].tracers;
+            if (p->neighbours != p0->neighbours || p->smoothness != p0->smoothness) continue;
+        }
+        TracerSet ts;
+        memset(&ts, 0, sizeof(ts));
+        ts.pp = pparams(p, en.dt, 1);
+        ts.step_idx = p->step_idx;
+        ts.ru = en.ctx->ru;
+        ts.pos = p->pos;
+        ts.hist = p->hist;
+        sets.push_back(ts);
+        start.push_back(start.back() + p->n);
+        e->batched.push_back(i);
+    }
+    if (!sets.empty()) {
+        if (cudaMalloc(&e->dsets, sets.size() * sizeof(TracerSet)) != cudaSuccess ||
+            cudaMalloc(&e->dstart, start.size() * sizeof(int64_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return ens_fail(e, BFG_ENOMEM, "cannot allocate tracer sets");
+        }
+        if (cudaMemcpy(e->dsets, sets.data(), sets.size() * sizeof(TracerSet), cudaMemcpyHostToDevice) !=
+                cudaSuccess ||
+            cudaMemcpy(e->dstart, start.data(), start.size() * sizeof(int64_t), cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+            return ens_fail(e, BFG_ECUDA, "tracer set upload failed");
+        e->nbatched = start.back();
+    }
     e->dirty = false;
     return 0;
 }
@@ -1616,10 +1687,26 @@ int bfg_ens_step(bfg_ens* e, int nsteps) {
             if (rc) return ens_fail(e, rc, "stage 1 launch failed");
         }
         if (cudaEventRecord(e->ev_ru, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
-        for (auto& en : e->entries) {
+        if (!e->batched.empty()) {
+            bfg_pctx* p0 = e->entries[e->batched[0]].tracers;
+            rc = e->real_bytes == 4 ? ens_tracers_dispatch<float>(e, p0->neighbours, p0->smoothness)
+                                    : ens_tracers_dispatch<double>(e, p0->neighbours, p0->smoothness);
+            if (rc) return ens_fail(e, rc, "batched tracer launch failed");
+            for (int i : e->batched) {
+                // host mirror of tracer_sets_advance
+                bfg_pctx* p = e->entries[i].tracers;
+                p->step_idx += 1;
+                p->head = (p->head - 1 + p->nsteps) % p->nsteps;
+                p->rhs0_zero = true;
+            }
+        }
+        for (int i = 0; i < (int)e->entries.size(); ++i) {
+            auto& en = e->entries[i];
             if (!en.tracers) continue;
             bfg_ctx* c = en.ctx;
-            if ((rc = tracer_loop(en.tracers, en.dt, e->stream))) return ens_fail(e, rc, c->err.c_str());
+            if (std::find(e->batched.begin(), e->batched.end(), i) == e->batched.end() &&
+                (rc = tracer_loop(en.tracers, en.dt, e->stream)))
+                return ens_fail(e, rc, c->err.c_str());
             if (cudaEventRecord(c->ev_tr, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
         }
         for (int s = 1; s < 3; ++s)

@@ -118,13 +118,12 @@ __device__ __forceinline__ void row_accumulate(const T* __restrict__ row, int x0
 
 constexpr int TRACER_THREADS = 128;
 
+// tracer i of one system: gather u(x_i), then (move) the Adams-Bashforth step
 template <typename T, int NB, int MM>
-__global__ void __launch_bounds__(TRACER_THREADS)
-tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ pos,
-              double* __restrict__ hist, double* __restrict__ sample_out) {
+__device__ __forceinline__ void tracer_one(const PParams& pp, const T* __restrict__ ru,
+                                           double* __restrict__ pos, double* __restrict__ hist,
+                                           double* __restrict__ sample_out, int64_t i) {
     constexpr int NP = 2 * NB + 2;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pp.n) return;
     const int N = pp.N;
     double p[3];
     int g[3];
@@ -203,6 +202,52 @@ tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ p
         }
         pos[i * 3 + d] = x;
     }
+}
+
+template <typename T, int NB, int MM>
+__global__ void __launch_bounds__(TRACER_THREADS)
+tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ pos,
+              double* __restrict__ hist, double* __restrict__ sample_out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pp.n) return;
+    tracer_one<T, NB, MM>(pp, ru, pos, hist, sample_out, i);
+}
+
+// the tracer systems of many ensemble members in one launch: thread i
+// belongs to the member k with start[k] <= i < start[k+1]
+struct TracerSet {
+    PParams pp;     // head, order and accum advance on the device after each loop
+    int step_idx;
+    const void* ru;
+    double* pos;
+    double* hist;
+};
+
+// inc_step_idx + shift_rhs_vectors of every set (particles_system.hpp:191-208)
+__global__ void tracer_sets_advance(TracerSet* __restrict__ sets, int nsets) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nsets) return;
+    TracerSet& s = sets[k];
+    s.step_idx += 1;
+    s.pp.head = (s.pp.head - 1 + s.pp.nsteps) % s.pp.nsteps;
+    s.pp.order = min(s.step_idx, s.pp.nsteps);
+    s.pp.accum = 0;
+}
+
+template <typename T, int NB, int MM>
+__global__ void __launch_bounds__(TRACER_THREADS)
+tracer_batch_kernel(const TracerSet* __restrict__ sets, const int64_t* __restrict__ start,
+                    int nsets) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= start[nsets]) return;
+    int lo = 0, hi = nsets - 1;
+    while (lo < hi) {  // last k with start[k] <= i
+        const int mid = (lo + hi + 1) / 2;
+        if (start[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    const TracerSet& s = sets[lo];
+    tracer_one<T, NB, MM>(s.pp, (const T*)s.ru, s.pos, s.hist, nullptr, i - start[lo]);
 }
 
 // ---------------------------------------------------------------------------

@@ -337,17 +337,24 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                                    min(TKX, NXV - kx0), nxp3, tid);
     }
     cp_async_commit();
+    __shared__ Member<T> mb;  // this tile's member, read once per tile
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
         cpx<T>* tile = bufs + (it & 1) * TILE;
         const int m = t / tiles_per, tl = t - m * tiles_per;
-        const Member<T>& mb = mem[m];
+        {
+            // the previous tile ended with a barrier: nobody reads mb now
+            constexpr int NWORDS = (int)(sizeof(Member<T>) / sizeof(int));
+            const int* src = reinterpret_cast<const int*>(&mem[m]);
+            int* dst = reinterpret_cast<int*>(&mb);
+            for (int i = tid; i < NWORDS; i += COL_THREADS) dst[i] = src[i];
+        }
         if constexpr (NRK > 0) {
             // RK operands of this tile: rows S[ky=a][kz=l], streamed while the
             // tile is transformed (the epilogue of the previous tile is done)
             const int a = tl / ntx;
             const int kx0 = (tl % ntx) * TKX;
-            const cpx<T>* rk_v0 = mbuf(mb, rl.v0);
-            const cpx<T>* rk_vp = mbuf(mb, rl.vp);
+            const cpx<T>* rk_v0 = mbuf(mem[m], rl.v0);  // mb is not yet visible to all
+            const cpx<T>* rk_vp = mbuf(mem[m], rl.vp);
             const int nvalid = (3 * min(TKX, NXV - kx0) + VPE - 1) / VPE;
             for (int e = tid; e < N * NRK * WV; e += COL_THREADS) {
                 const int v = e % WV;
@@ -464,6 +471,8 @@ enum RowMode {
     RM_R2C = 2,        // real rows -> complex rows
 };
 constexpr int ROW_THREADS = 512;
+constexpr int ROW_CTAS = 1;  // resident CTAs per SM
+constexpr int ROW_BUDGET = SMEM_BUDGET / ROW_CTAS - 2048;
 
 template <int N>
 __host__ __device__ constexpr int row_rl() { return (N / 2 + 4) * 3; }  // padded row, complex
@@ -482,7 +491,7 @@ __host__ __device__ constexpr size_t row_bytes_for(int R) {
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int row_rows_from(int R) {
-    return (R <= 1 || (row_bytes_for<T, N, MODE>(R) <= (size_t)SMEM_BUDGET && R <= (N * N) / 296))
+    return (R <= 1 || (row_bytes_for<T, N, MODE>(R) <= (size_t)ROW_BUDGET && R <= (N * N) / 296))
                ? (R < 1 ? 1 : R)
                : row_rows_from<T, N, MODE>(R / 2);
 }
@@ -582,7 +591,7 @@ __device__ __forceinline__ void row_issue_load(cpx<T>* stage, const cpx<T>* wu, 
 }
 
 template <typename T, int N, int MODE, bool WRITE_RU>
-__global__ void __launch_bounds__(ROW_THREADS, 1)
+__global__ void __launch_bounds__(ROW_THREADS, ROW_CTAS)
 row_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
          int tiles_per, int ntiles) {
     constexpr int M = N / 2;
