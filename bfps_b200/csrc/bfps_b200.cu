@@ -239,6 +239,21 @@ struct Engine {
     // one persistent launch of a row pass over nmem members
     template <int MODE, bool WRU>
     static int row(bfg_ctx* c, const Mem* mem, int nmem, Roles rl) {
+        if constexpr (MODE == RM_NONLIN && rnl_fused<N>()) {
+            constexpr size_t smem = rnl_smem_bytes<T, N>();
+            constexpr int ROWS = rnl_rows<T, N>();
+            auto kern = row_nonlin<T, N, WRU>;
+            if (smem > (size_t)c->smem_optin)
+                return fail(c, BFG_EUNSUP, "row pass needs %zu bytes of shared memory", smem);
+            CU(ensure_smem(kern, smem, c->device));
+            const int tiles_per = N * N / ROWS;
+            const int ntiles = tiles_per * nmem;
+            const int grid = std::min(ntiles, c->nsm);
+            Prof pr(c, K_X);
+            kern<<<grid, ROW_THREADS, smem, c->stream>>>(mem, rl, (const C*)c->tw, tiles_per,
+                                                         ntiles);
+            return after_launch(c, "row_nonlin");
+        }
         constexpr size_t smem = row_smem_bytes<T, N, MODE>();
         constexpr int ROWS = row_rows<T, N, MODE>();
         auto kern = row_pass<T, N, MODE, WRU>;

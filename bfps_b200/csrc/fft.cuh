@@ -288,6 +288,15 @@ __device__ __forceinline__ void dit_down(cpx<T>* s, const cpx<T>* tw, int tid, i
         dit_down<T, L, S - 1, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
     }
 }
+// DIT stages S down to SLO (inclusive), each followed by a barrier.
+template <typename T, int L, int S, int SLO, bool INV, int P, class LAY, int MAP, int TAB>
+__device__ __forceinline__ void dit_range(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {
+    if constexpr (S >= SLO) {
+        dit_stage<T, L, S, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
+        __syncthreads();
+        dit_range<T, L, S - 1, SLO, INV, P, LAY, MAP, TAB>(s, tw, tid, nthr);
+    }
+}
 // Full DIT transform: digit-reversed in, natural out.  Ends with a barrier.
 template <typename T, int L, bool INV, int P, class LAY, int MAP, int TAB>
 __device__ __forceinline__ void dit(cpx<T>* s, const cpx<T>* tw, int tid, int nthr) {

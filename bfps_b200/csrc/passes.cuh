@@ -727,6 +727,423 @@ row_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
 }
 
 // ---------------------------------------------------------------------------
+// Fused nonlinear row pass (the X pass of every RK stage, N >= 32).
+//
+// Same result as row_pass<RM_NONLIN> with fewer shared-memory round trips:
+//   A  C2R pre-processing fused with DIF stage 0: a work unit takes the
+//      butterflies j and S0 - j of stage 0 (span S0), whose inputs are each
+//      other's mirror partners k, M - k, straight from the staging rows;
+//   B  the middle DIF stages;
+//   C  the last DIF stage (span 1) of the six pencils of a row, u x w / N^3
+//      and the first DIT stage, in registers, per block of the last radix;
+//   D  the middle DIT stages;
+//   E  DIT stage 0 fused with the R2C post-processing, again on mirror
+//      pairs, writing interleaved output rows.
+// One staging buffer: the rows of the next tile stream in (cp.async) from
+// the end of phase A, while B..E and the store of this tile run.  Per row
+// the pencil region holds the u pencils (overwritten by the output row in
+// phase E) and the w pencils (which receive the product).  Pitches: the
+// region length RG is odd (-1 modulo the banks a wavefront spans), the
+// pencil pitch PL and the w offset W are multiples of the rows per tile
+// modulo that count, so that lanes on (pencil, row) or (block, row) pairs
+// hit distinct banks.
+template <typename T>
+__host__ __device__ constexpr int nslot() { return 128 / (int)sizeof(cpx<T>); }
+// smallest x >= v with x = res (mod md)
+__host__ __device__ constexpr int at_least_mod(int v, int md, int res) {
+    return v + (((res - v) % md) + md) % md;
+}
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_pl(int R) {
+    return at_least_mod(N / 2 + 1, nslot<T>(), R % nslot<T>());
+}
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_w(int R) {
+    return at_least_mod(row_rl<N>() > 2 * rnl_pl<T, N>(R) + N / 2 ? row_rl<N>()
+                                                                  : 2 * rnl_pl<T, N>(R) + N / 2,
+                        nslot<T>(), (3 * R) % nslot<T>());
+}
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_rg(int R) {
+    return at_least_mod(rnl_w<T, N>(R) + 3 * rnl_pl<T, N>(R), nslot<T>(), nslot<T>() - 1);
+}
+template <int N>
+__host__ __device__ constexpr int rnl_tw0() {
+    return (N / 2) / plan_radix(N / 2, 0) * (plan_radix(N / 2, 0) - 1);
+}
+template <typename T, int N>
+__host__ __device__ constexpr size_t rnl_bytes_for(int R) {
+    return (size_t)(2 * R * row_rl<N>() + R * rnl_rg<T, N>(R) + N + rnl_tw0<N>()) *
+               sizeof(cpx<T>) +
+           (size_t)(N / 2) * 4;
+}
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_rows_from(int R) {
+    return (R <= 1 || (rnl_bytes_for<T, N>(R) <= (size_t)ROW_BUDGET && R <= (N * N) / 296))
+               ? (R < 1 ? 1 : R)
+               : rnl_rows_from<T, N>(R / 2);
+}
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_rows() { return rnl_rows_from<T, N>(16); }
+template <typename T, int N>
+__host__ __device__ constexpr size_t rnl_smem_bytes() {
+    return rnl_bytes_for<T, N>(rnl_rows<T, N>());
+}
+template <int N>
+__host__ __device__ constexpr bool rnl_fused() { return plan_nstages(N / 2) >= 2; }
+
+// pencil p = c6 * ROWS + r: c6 < 3 the u pencils, c6 >= 3 the w pencils
+template <int ROWS, int RG, int PL, int W>
+struct LayNL6 {
+    static constexpr int ES = 1;
+    __device__ __forceinline__ static int base(int p) {
+        const int c6 = p / ROWS, r = p - c6 * ROWS;
+        return r * RG + (c6 < 3 ? c6 * PL : W + (c6 - 3) * PL);
+    }
+};
+// the w pencils only: p = c * ROWS + r
+template <int ROWS, int RG, int PL, int W>
+struct LayNLW {
+    static constexpr int ES = 1;
+    __device__ __forceinline__ static int base(int p) {
+        const int c = p / ROWS, r = p - c * ROWS;
+        return r * RG + W + c * PL;
+    }
+};
+
+// C2R pre-processing of one mirror pair held in registers: a = X[k],
+// b = X[M-k] become Z[k], Z[M-k] (w = exp(-2 pi i k / N)); the formulas of
+// c2r_pre.
+template <typename T>
+__device__ __forceinline__ cpx<T> c2r_lo(cpx<T> a, cpx<T> b, cpx<T> w) {
+    const cpx<T> sp = a + conjg(b), dm = a - conjg(b);
+    const cpx<T> e = cmulc(dm, w);
+    return mk<T>(sp.x - e.y, sp.y + e.x);
+}
+template <typename T>
+__device__ __forceinline__ cpx<T> c2r_hi(cpx<T> a, cpx<T> b, cpx<T> w) {
+    const cpx<T> sp = b + conjg(a), dm = b - conjg(a);
+    const cpx<T> e = cmul(dm, w);
+    return mk<T>(sp.x + e.y, sp.y - e.x);
+}
+// R2C post-processing of one mirror pair: zk = Z[k], zm = Z[M-k] give X[k]
+// and X[M-k]; the formulas of r2c_post.
+template <typename T>
+__device__ __forceinline__ cpx<T> r2c_lo(cpx<T> zk, cpx<T> zm, cpx<T> w) {
+    const T h = (T)0.5;
+    const cpx<T> e = scale(zk + conjg(zm), h);
+    const cpx<T> d = zk - conjg(zm);
+    const cpx<T> o = mk<T>(d.y * h, -d.x * h);
+    return e + cmul(w, o);
+}
+template <typename T>
+__device__ __forceinline__ cpx<T> r2c_hi(cpx<T> zk, cpx<T> zm, cpx<T> w) {
+    const T h = (T)0.5;
+    const cpx<T> e = scale(zm + conjg(zk), h);
+    const cpx<T> d = zm - conjg(zk);
+    const cpx<T> o = mk<T>(d.y * h, -d.x * h);
+    return e - cmul(conjg(w), o);
+}
+
+template <typename T, int N, bool WRITE_RU>
+__global__ void __launch_bounds__(ROW_THREADS, 1)
+row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
+           int tiles_per, int ntiles) {
+    constexpr int M = N / 2;
+    constexpr int NS = plan_nstages(M);
+    constexpr int R0 = plan_radix(M, 0);
+    constexpr int S0 = M / R0;                 // span of stage 0
+    constexpr int H0 = S0 / 2;                 // mirror-paired units per pencil
+    constexpr int RZ = plan_radix(M, NS - 1);  // radix of the last stage (span 1)
+    constexpr int NBZ = M / RZ;
+    constexpr int ROWS = rnl_rows<T, N>();
+    constexpr int RL = row_rl<N>();
+    constexpr int PL = rnl_pl<T, N>(ROWS);
+    constexpr int W = rnl_w<T, N>(ROWS);
+    constexpr int RG = rnl_rg<T, N>(ROWS);
+    constexpr int VPE = 16 / (int)sizeof(cpx<T>);
+    constexpr int NV = ROWS * RL / VPE;        // 16-byte vectors per input buffer
+    constexpr int G = (ROWS % RZ == 0) ? RZ : ROWS;  // rows across lanes in phase C
+    constexpr bool SPLIT = RZ * 6 * (int)sizeof(cpx<T>) > 192;  // w's last stage apart
+    using L6 = LayNL6<ROWS, RG, PL, W>;
+    using LW = LayNLW<ROWS, RG, PL, W>;
+    static_assert(NS >= 2 && H0 >= 2, "fused row pass needs two stages");
+    static_assert(W >= RL && W >= 2 * PL + M && (RG & 1), "region layout");
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* st = reinterpret_cast<cpx<T>*>(smem_raw);  // u rows, then w rows
+    cpx<T>* P = st + 2 * ROWS * RL;                     // ROWS regions of RG
+    cpx<T>* tw = P + ROWS * RG;
+    cpx<T>* tw0 = tw + N;  // stage-0 twiddles [j][q-1] = tw[2 j q]
+    int* posn = reinterpret_cast<int*>(tw0 + rnl_tw0<N>());
+    const int tid = threadIdx.x;
+
+    for (int i = tid; i < N; i += ROW_THREADS) tw[i] = tw_g[i];
+    for (int i = tid; i < rnl_tw0<N>(); i += ROW_THREADS) {
+        const int j = i / (R0 - 1), q = i - j * (R0 - 1) + 1;
+        tw0[i] = tw_g[2 * j * q];
+    }
+    if constexpr (WRITE_RU)
+        for (int i = tid; i < M; i += ROW_THREADS) posn[i] = dif_position<M>(i);
+
+    auto issue = [&](int tt) {
+        const int mm = tt / tiles_per, tl = tt - mm * tiles_per;
+        const cpx<T>* su = mbuf(mem[mm], rl.in0) + (size_t)tl * ROWS * RL;
+        const cpx<T>* sw = mbuf(mem[mm], rl.in1) + (size_t)tl * ROWS * RL;
+        for (int e = tid; e < 2 * NV; e += ROW_THREADS) {
+            const int b = e >= NV ? 1 : 0;
+            const int v = e - b * NV;
+            cp_async16(&st[b * ROWS * RL + v * VPE], &(b ? sw : su)[v * VPE]);
+        }
+    };
+    int t = blockIdx.x;
+    if (t < ntiles) issue(t);
+    cp_async_commit();
+    for (; t < ntiles; t += gridDim.x) {
+        cp_async_wait<0>();
+        __syncthreads();
+        const int m = t / tiles_per, tl = t - m * tiles_per;
+        const size_t row0 = (size_t)tl * ROWS;
+
+        // A: C2R pre-processing + DIF stage 0, staging rows -> pencils
+        for (int e = tid; e < 6 * ROWS * H0; e += ROW_THREADS) {
+            const int u = e % H0;
+            const int p = e / H0;  // = r * 6 + c6
+            const int r = p / 6, c6 = p - 6 * r;
+            const int b = c6 >= 3 ? 1 : 0, c = c6 - 3 * b;
+            const cpx<T>* x = st + (b * ROWS + r) * RL + c;
+            cpx<T>* z = P + r * RG + (b ? W : 0) + c * PL;
+            const int ja = u, jb = u == 0 ? H0 : S0 - u;
+            cpx<T> va[R0], vb[R0];
+#pragma unroll
+            for (int q = 0; q < R0; ++q) {
+                va[q] = x[3 * (ja + S0 * q)];
+                vb[q] = x[3 * (jb + S0 * q)];
+            }
+            if (u != 0) {
+                // k = u + S0 q pairs with M - k = jb + S0 (R0 - 1 - q)
+#pragma unroll
+                for (int q = 0; q < R0 / 2; ++q) {
+                    const cpx<T> a0 = va[q], b0 = vb[R0 - 1 - q];
+                    const cpx<T> a1 = va[R0 - 1 - q], b1 = vb[q];
+                    const cpx<T> w0 = tw[ja + S0 * q], w1 = tw[ja + S0 * (R0 - 1 - q)];
+                    va[q] = c2r_lo(a0, b0, w0);
+                    vb[R0 - 1 - q] = c2r_hi(a0, b0, w0);
+                    va[R0 - 1 - q] = c2r_lo(a1, b1, w1);
+                    vb[q] = c2r_hi(a1, b1, w1);
+                }
+            } else {
+                // item 0: k = S0 q pairs with S0 (R0 - q); X[0] with X[M]
+                const T x0 = va[0].x, xm = x[3 * M].x;
+                va[0] = mk<T>(x0 + xm, x0 - xm);
+#pragma unroll
+                for (int q = 1; q < R0 / 2; ++q) {
+                    const cpx<T> a0 = va[q], b0 = va[R0 - q];
+                    const cpx<T> w0 = tw[S0 * q];
+                    va[q] = c2r_lo(a0, b0, w0);
+                    va[R0 - q] = c2r_hi(a0, b0, w0);
+                }
+                va[R0 / 2] = c2r_lo(va[R0 / 2], va[R0 / 2], tw[S0 * (R0 / 2)]);
+                // item S0/2: k = H0 + S0 q pairs with H0 + S0 (R0 - 1 - q)
+#pragma unroll
+                for (int q = 0; q < R0 / 2; ++q) {
+                    const cpx<T> a0 = vb[q], b0 = vb[R0 - 1 - q];
+                    const cpx<T> w0 = tw[H0 + S0 * q];
+                    vb[q] = c2r_lo(a0, b0, w0);
+                    vb[R0 - 1 - q] = c2r_hi(a0, b0, w0);
+                }
+            }
+            dft<T, true, R0>(va);
+            dft<T, true, R0>(vb);
+#pragma unroll
+            for (int q = 1; q < R0; ++q) {
+                va[q] = cmulc(va[q], tw0[ja * (R0 - 1) + q - 1]);
+                vb[q] = cmulc(vb[q], tw0[jb * (R0 - 1) + q - 1]);
+            }
+#pragma unroll
+            for (int q = 0; q < R0; ++q) {
+                z[ja + S0 * q] = va[q];
+                z[jb + S0 * q] = vb[q];
+            }
+        }
+        __syncthreads();
+        // the staging rows are free: stream in the next tile
+        if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
+        cp_async_commit();
+
+        // B: middle DIF stages over the six pencils of each row
+        dif_range<T, M, 1, NS - 1, true, 6 * ROWS, L6, 2, N>(P, tw, tid, ROW_THREADS);
+        if constexpr (SPLIT) {
+            dif_stage<T, M, NS - 1, true, 3 * ROWS, LW, 2, N>(P, tw, tid, ROW_THREADS);
+            __syncthreads();
+        }
+
+        // C: last DIF stage, u x w / N^3, first DIT stage (product -> w pencils)
+        {
+            const T inv_np = (T)1 / ((T)N * (T)N * (T)N);
+            for (int e = tid; e < ROWS * NBZ; e += ROW_THREADS) {
+                const int rlo = e % G;
+                const int t2 = e / G;
+                const int bb = t2 % NBZ;
+                const int r = (t2 / NBZ) * G + rlo;
+                cpx<T>* reg = P + r * RG + bb * RZ;
+                cpx<T> uu[3][RZ];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+#pragma unroll
+                    for (int q = 0; q < RZ; ++q) uu[c][q] = reg[c * PL + q];
+                    dft<T, true, RZ>(uu[c]);
+                }
+                if constexpr (WRITE_RU) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int q = 0; q < RZ; ++q) reg[c * PL + q] = uu[c][q];
+                }
+                if constexpr (SPLIT) {
+#pragma unroll
+                    for (int q = 0; q < RZ; ++q) {
+                        cpx<T> w3[3];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) w3[c] = reg[W + c * PL + q];
+                        cpx<T> pr[3];
+#pragma unroll
+                        for (int cc = 0; cc < 3; ++cc) {
+                            const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+                            const T tx = uu[c1][q].x * w3[c2].x - uu[c2][q].x * w3[c1].x;
+                            const T ty = uu[c1][q].y * w3[c2].y - uu[c2][q].y * w3[c1].y;
+                            pr[cc] = mk<T>(tx * inv_np, ty * inv_np);
+                        }
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) uu[c][q] = pr[c];
+                    }
+                } else {
+                    cpx<T> ww[3][RZ];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+                        for (int q = 0; q < RZ; ++q) ww[c][q] = reg[W + c * PL + q];
+                        dft<T, true, RZ>(ww[c]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < RZ; ++q) {
+                        cpx<T> pr[3];
+#pragma unroll
+                        for (int cc = 0; cc < 3; ++cc) {
+                            const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+                            const T tx = uu[c1][q].x * ww[c2][q].x - uu[c2][q].x * ww[c1][q].x;
+                            const T ty = uu[c1][q].y * ww[c2][q].y - uu[c2][q].y * ww[c1][q].y;
+                            pr[cc] = mk<T>(tx * inv_np, ty * inv_np);
+                        }
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) uu[c][q] = pr[c];
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    dft<T, false, RZ>(uu[c]);
+#pragma unroll
+                    for (int q = 0; q < RZ; ++q) reg[W + c * PL + q] = uu[c][q];
+                }
+            }
+        }
+        __syncthreads();
+        if constexpr (WRITE_RU) {
+            // real u (u pencils after the inverse transform) in natural x order
+            T* rout = mreal(mem[m], rl.rout);
+            for (int e = tid; e < ROWS * N * 3; e += ROW_THREADS) {
+                const int c = e % 3;
+                const int r2 = e / 3;
+                const int xx = r2 % N;
+                const int r = r2 / N;
+                const cpx<T> z = P[r * RG + c * PL + posn[xx >> 1]];
+                rout[(row0 + r) * (N * 3) + xx * 3 + c] = (xx & 1) ? z.y : z.x;
+            }
+            if constexpr (NS == 2) __syncthreads();  // phase E overwrites the u pencils
+        }
+
+        // D: middle DIT stages over the w pencils
+        dit_range<T, M, NS - 2, 1, false, 3 * ROWS, LW, 2, N>(P, tw, tid, ROW_THREADS);
+
+        // E: DIT stage 0 + R2C post-processing, w pencils -> output rows
+        for (int e = tid; e < 3 * ROWS * H0; e += ROW_THREADS) {
+            const int u = e % H0;
+            const int p = e / H0;  // = r * 3 + c
+            const int r = p / 3, c = p - 3 * r;
+            const cpx<T>* z = P + r * RG + W + c * PL;
+            cpx<T>* x = P + r * RG + c;
+            const int ja = u, jb = u == 0 ? H0 : S0 - u;
+            cpx<T> va[R0], vb[R0];
+#pragma unroll
+            for (int q = 0; q < R0; ++q) {
+                va[q] = z[ja + S0 * q];
+                vb[q] = z[jb + S0 * q];
+            }
+#pragma unroll
+            for (int q = 1; q < R0; ++q) {
+                va[q] = cmul(va[q], tw0[ja * (R0 - 1) + q - 1]);
+                vb[q] = cmul(vb[q], tw0[jb * (R0 - 1) + q - 1]);
+            }
+            dft<T, false, R0>(va);
+            dft<T, false, R0>(vb);
+            if (u != 0) {
+#pragma unroll
+                for (int q = 0; q < R0; ++q) {
+                    const int k = ja + S0 * q;
+                    const cpx<T> w0 = tw[k];
+                    x[3 * k] = r2c_lo(va[q], vb[R0 - 1 - q], w0);
+                    x[3 * (M - k)] = r2c_hi(va[q], vb[R0 - 1 - q], w0);
+                }
+            } else {
+                const cpx<T> z0 = va[0];
+                x[0] = mk<T>(z0.x + z0.y, (T)0);
+                x[3 * M] = mk<T>(z0.x - z0.y, (T)0);
+#pragma unroll
+                for (int q = 1; q < R0 / 2; ++q) {
+                    const int k = S0 * q;
+                    const cpx<T> w0 = tw[k];
+                    x[3 * k] = r2c_lo(va[q], va[R0 - q], w0);
+                    x[3 * (M - k)] = r2c_hi(va[q], va[R0 - q], w0);
+                }
+                x[3 * (M / 2)] = r2c_lo(va[R0 / 2], va[R0 / 2], tw[M / 2]);
+#pragma unroll
+                for (int q = 0; q < R0 / 2; ++q) {
+                    const int k = H0 + S0 * q;
+                    const cpx<T> w0 = tw[k];
+                    x[3 * k] = r2c_lo(vb[q], vb[R0 - 1 - q], w0);
+                    x[3 * (M - k)] = r2c_hi(vb[q], vb[R0 - 1 - q], w0);
+                }
+            }
+        }
+        // padding points of the output rows carry zeros
+        for (int i = tid; i < ROWS * (RL - 3 * (M + 1)); i += ROW_THREADS) {
+            const int r = i / (RL - 3 * (M + 1));
+            P[r * RG + 3 * (M + 1) + (i - r * (RL - 3 * (M + 1)))] = zero_c<T>();
+        }
+        __syncthreads();
+        // output rows out with 16-byte vectors
+        {
+            cpx<T>* wout = mbuf(mem[m], rl.out0) + row0 * RL;
+            float4* dst = reinterpret_cast<float4*>(wout);
+            for (int v = tid; v < NV; v += ROW_THREADS) {
+                const int r = v / (RL / VPE);
+                const cpx<T>* s = P + r * RG + (v - r * (RL / VPE)) * VPE;
+                float4 val;
+                if constexpr (VPE == 2) {
+                    const cpx<T> a = s[0], b = s[1];
+                    val = make_float4(a.x, a.y, b.x, b.y);
+                } else {
+                    val = *reinterpret_cast<const float4*>(s);
+                }
+                dst[v] = val;
+            }
+        }
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
 // field::symmetrize on the kx = 0 plane of a state-layout buffer
 // (field.cpp:903-978).  One thread per (ky, kz) of the plane.
 template <typename T, int N>
