@@ -636,8 +636,16 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=None,
+                    help="override the workload's grid size N (profiling cases)")
+    ap.add_argument("--tracers", type=int, default=None,
+                    help="override the workload's tracer count (profiling cases)")
     args = ap.parse_args()
-    cfg = WORKLOADS[args.workload]
+    cfg = dict(WORKLOADS[args.workload])
+    if args.grid is not None:
+        cfg["n"] = args.grid
+    if args.tracers is not None:
+        cfg["ntracers"] = args.tracers
     if args.impl == "reference":
         run_reference(args, cfg)
     elif cfg.get("kind") == "ensemble":

@@ -807,44 +807,59 @@ int bfg_kspace_info(const bfg_ctx* c, double* kM, double* dk, int* nshells, doub
     return 0;
 }
 
+// Pitched row copy on the device, 8-byte words: rows of wq words from a
+// source of pitch sq to a destination of pitch dq; the zq words after each
+// destination row are set to zero.
+__global__ void pitch_copy8(const uint2* __restrict__ src, size_t sq, uint2* __restrict__ dst,
+                            size_t dq, int wq, int zq, size_t rows) {
+    for (size_t r = blockIdx.x; r < rows; r += gridDim.x) {
+        for (int k = threadIdx.x; k < wq; k += blockDim.x) dst[r * dq + k] = src[r * sq + k];
+        for (int k = threadIdx.x; k < zq; k += blockDim.x) dst[r * dq + wq + k] = make_uint2(0, 0);
+    }
+}
+
+// Host <-> device field transfer.  The host side is the reference layout;
+// the copy itself is one contiguous transfer through the scratch buffer wb
+// (pitched host copies run well below the link rate), the change of row
+// pitch is a device kernel.
 static int field_copy(bfg_ctx* c, int field_id, void* host, bool upload) {
     if (!c || !host) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
     if (int rj = join_tracers(c)) return rj;
     const size_t cb = 2 * (size_t)c->real_bytes;
     const size_t N = c->n;
+    const size_t rows = N * N;
+    size_t dpitch, hpitch, width;  // bytes
+    void* dev;
     if (field_id == BFG_FIELD_VORTICITY || field_id == BFG_FIELD_VELOCITY) {
-        void* dev = field_id == BFG_FIELD_VORTICITY ? c->w0 : c->wa;
-        const size_t dpitch = (size_t)c->nxp * 3 * cb, hpitch = (size_t)c->nxv * 3 * cb;
-        if (upload)
-            CU(cudaMemcpy2DAsync(dev, dpitch, host, hpitch, hpitch, N * N, cudaMemcpyHostToDevice,
-                                 c->stream));
-        else
-            CU(cudaMemcpy2DAsync(host, hpitch, dev, dpitch, hpitch, N * N, cudaMemcpyDeviceToHost,
-                                 c->stream));
-        CU(cudaStreamSynchronize(c->stream));
-        return 0;
-    }
-    if (field_id == BFG_FIELD_RVELOCITY) {
+        dev = field_id == BFG_FIELD_VORTICITY ? c->w0 : c->wa;
+        dpitch = (size_t)c->nxp * 3 * cb;
+        hpitch = width = (size_t)c->nxv * 3 * cb;
+    } else if (field_id == BFG_FIELD_RVELOCITY) {
         int rc = ensure_ru(c);
         if (rc) return rc;
         const size_t rb = c->real_bytes;
-        const size_t dpitch = N * 3 * rb, hpitch = (N + 2) * 3 * rb;
-        if (upload) {
-            CU(cudaMemcpy2DAsync(c->ru, dpitch, host, hpitch, dpitch, N * N, cudaMemcpyHostToDevice,
-                                 c->stream));
-        } else {
-            CU(cudaMemcpy2DAsync(host, hpitch, c->ru, dpitch, dpitch, N * N, cudaMemcpyDeviceToHost,
-                                 c->stream));
-        }
-        CU(cudaStreamSynchronize(c->stream));
-        if (!upload) {
-            for (size_t r = 0; r < N * N; ++r)
-                memset((char*)host + r * hpitch + dpitch, 0, hpitch - dpitch);
-        }
-        return 0;
+        dev = c->ru;
+        dpitch = width = N * 3 * rb;
+        hpitch = (N + 2) * 3 * rb;
+    } else {
+        return fail(c, BFG_EINVAL, "unknown field id %d", field_id);
     }
-    return fail(c, BFG_EINVAL, "unknown field id %d", field_id);
+    const int grid = c->nsm * 8;
+    const int wq = (int)(width / 8);
+    if (upload) {
+        CU(cudaMemcpyAsync(c->wb, host, rows * hpitch, cudaMemcpyHostToDevice, c->stream));
+        pitch_copy8<<<grid, 256, 0, c->stream>>>((const uint2*)c->wb, hpitch / 8, (uint2*)dev,
+                                                 dpitch / 8, wq, 0, rows);
+        CU(cudaGetLastError());
+    } else {
+        pitch_copy8<<<grid, 256, 0, c->stream>>>((const uint2*)dev, dpitch / 8, (uint2*)c->wb,
+                                                 hpitch / 8, wq, (int)((hpitch - width) / 8), rows);
+        CU(cudaGetLastError());
+        CU(cudaMemcpyAsync(host, c->wb, rows * hpitch, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
 }
 
 int bfg_field_upload(bfg_ctx* c, int field_id, const void* host) {

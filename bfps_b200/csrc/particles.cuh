@@ -8,7 +8,8 @@
 //   particles_system::completeLoop (particles_system.hpp:210-217)
 // The weights, positions and accumulation are double; the field is read in
 // its storage precision and promoted, as in the reference.  The sum runs
-// z-outer, x-middle, y-inner like apply_computation.
+// as (b_z b_y) b_x f over z, then y, with x innermost along the contiguous
+// row (apply_computation runs z, x, y; the sums agree to rounding).
 //
 // The rhs history is a ring of nsteps slots: logical rhs[j] is slot
 // (head + j) % nsteps.  The host rotates `head` after each loop
@@ -116,6 +117,97 @@ __device__ __forceinline__ void row_accumulate(const T* __restrict__ row, int x0
     }
 }
 
+// FP32 field (precision form): the x sums of each stencil row run in FP32
+// with the x weights rounded to FP32; the y/z weights, the accumulation of
+// the row sums and everything after stay FP64.  Three conversions per row
+// instead of one per value.  A row segment is read as 16-byte vectors from
+// its aligned-down start; instead of shifting the loaded words, the x
+// weights are shifted once per tracer (word i of the aligned block belongs to
+// point (i - off) / 3, component (i - off) mod 3) and the sums are kept per
+// word phase i mod 3, mapped to components at the end.
+template <int NB>
+__device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int N, const int* g,
+                                               int x0, const double* wx, const double* wy,
+                                               const double* wz, double& a0, double& a1,
+                                               double& a2) {
+    constexpr int NP = 2 * NB + 2;
+    constexpr int NV = (3 * NP + 3) / 4 + 1;  // vectors covering any alignment
+    constexpr int NF = 4 * NV;
+    const size_t rowN = (size_t)N;
+    float wxf[NP];
+#pragma unroll
+    for (int ix = 0; ix < NP; ++ix) wxf[ix] = (float)wx[ix];
+    if (x0 >= 0 && x0 + NP <= N) {
+        const int e0 = x0 * 3;
+        const int base = e0 & ~3;
+        const int off = e0 - base;
+        const int maxv = (N * 3 - base) / 4;  // vectors left in the row
+        float wt[NF];
+#pragma unroll
+        for (int i = 0; i < NF; ++i) {
+            float w = 0.f;
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+                const int k = i - o;
+                if (k >= 0 && k < 3 * NP) w = (off == o) ? wxf[k / 3] : w;
+            }
+            wt[i] = w;
+        }
+        double ph[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int iz = 0; iz < NP; ++iz) {
+            const int z = (g[2] - NB + iz + N) % N;
+#pragma unroll 1
+            for (int iy = 0; iy < NP; ++iy) {
+                const int y = (g[1] - NB + iy + N) % N;
+                const float* row = ru + ((size_t)z * rowN + y) * rowN * 3 + base;
+                float sp[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    if (v < maxv) {
+                        const float4 q = *reinterpret_cast<const float4*>(row + 4 * v);
+                        sp[(4 * v + 0) % 3] = fmaf(q.x, wt[4 * v + 0], sp[(4 * v + 0) % 3]);
+                        sp[(4 * v + 1) % 3] = fmaf(q.y, wt[4 * v + 1], sp[(4 * v + 1) % 3]);
+                        sp[(4 * v + 2) % 3] = fmaf(q.z, wt[4 * v + 2], sp[(4 * v + 2) % 3]);
+                        sp[(4 * v + 3) % 3] = fmaf(q.w, wt[4 * v + 3], sp[(4 * v + 3) % 3]);
+                    }
+                }
+                const double bzy = wz[iz] * wy[iy];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) ph[k] = fma(bzy, (double)sp[k], ph[k]);
+            }
+        }
+        // component c sits in phase (c + off) mod 3
+        const int k0 = off % 3;
+        a0 = k0 == 0 ? ph[0] : (k0 == 1 ? ph[1] : ph[2]);
+        a1 = k0 == 0 ? ph[1] : (k0 == 1 ? ph[2] : ph[0]);
+        a2 = k0 == 0 ? ph[2] : (k0 == 1 ? ph[0] : ph[1]);
+    } else {
+        // stencil across the periodic x boundary: scalar loads
+#pragma unroll 1
+        for (int iz = 0; iz < NP; ++iz) {
+            const int z = (g[2] - NB + iz + N) % N;
+#pragma unroll 1
+            for (int iy = 0; iy < NP; ++iy) {
+                const int y = (g[1] - NB + iy + N) % N;
+                const float* row = ru + ((size_t)z * rowN + y) * rowN * 3;
+                float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll
+                for (int ix = 0; ix < NP; ++ix) {
+                    const int xx = (x0 + ix + N) % N;
+                    s0 = fmaf(row[xx * 3 + 0], wxf[ix], s0);
+                    s1 = fmaf(row[xx * 3 + 1], wxf[ix], s1);
+                    s2 = fmaf(row[xx * 3 + 2], wxf[ix], s2);
+                }
+                const double bzy = wz[iz] * wy[iy];
+                a0 = fma(bzy, (double)s0, a0);
+                a1 = fma(bzy, (double)s1, a1);
+                a2 = fma(bzy, (double)s2, a2);
+            }
+        }
+    }
+}
+
 constexpr int TRACER_THREADS = 128;
 
 // tracer i of one system: gather u(x_i), then (move) the Adams-Bashforth step
@@ -140,19 +232,24 @@ __device__ __forceinline__ void tracer_one(const PParams& pp, const T* __restric
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
     const size_t rowN = (size_t)N;
     const int x0 = g[0] - NB;
+    if constexpr (sizeof(T) == 4) {
+        row_gather_f32<NB>(reinterpret_cast<const float*>(ru), N, g, x0, wx, wy, wz, acc0, acc1,
+                           acc2);
+    } else {
 #pragma unroll 1
-    for (int iz = 0; iz < NP; ++iz) {
-        const int z = (g[2] - NB + iz + N) % N;
+        for (int iz = 0; iz < NP; ++iz) {
+            const int z = (g[2] - NB + iz + N) % N;
 #pragma unroll 1
-        for (int iy = 0; iy < NP; ++iy) {
-            const int y = (g[1] - NB + iy + N) % N;
-            // coefficient (bz * by) * bx of apply_computation
-            const double bzy = wz[iz] * wy[iy];
-            double wxc[NP];
+            for (int iy = 0; iy < NP; ++iy) {
+                const int y = (g[1] - NB + iy + N) % N;
+                // coefficient (bz * by) * bx of apply_computation
+                const double bzy = wz[iz] * wy[iy];
+                double wxc[NP];
 #pragma unroll
-            for (int ix = 0; ix < NP; ++ix) wxc[ix] = bzy * wx[ix];
-            row_accumulate<T, NB>(ru + ((size_t)z * rowN + y) * rowN * 3, x0, N, wxc, acc0, acc1,
-                                  acc2);
+                for (int ix = 0; ix < NP; ++ix) wxc[ix] = bzy * wx[ix];
+                row_accumulate<T, NB>(ru + ((size_t)z * rowN + y) * rowN * 3, x0, N, wxc, acc0,
+                                      acc1, acc2);
+            }
         }
     }
     if (!pp.move) {

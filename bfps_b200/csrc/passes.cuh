@@ -218,8 +218,11 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     curl<T>((T)kx, (T)ky, (T)kz, nl, tt);
     // forcing (vorticity_equation.cpp:241-288), factor 1
     if (kp.forcing == 1) {
-        const double kn = sqrt(k2);
-        if (kp.fk0 <= kn && kp.fk1 >= kn) {
+        // the band test on |k| = sqrt(k2), taken only where k2 is near the
+        // band (the margin keeps every mode the exact test accepts)
+        const double lo = kp.fk0 > 0.0 ? kp.fk0 * kp.fk0 * (1.0 - 1e-12) : -1.0;
+        const double hi = kp.fk1 * kp.fk1 * (1.0 + 1e-12);
+        if (k2 >= lo && k2 <= hi && kp.fk0 <= sqrt(k2) && kp.fk1 >= sqrt(k2)) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const cpx<T> fv = fsrc[pt * 3 + c];
@@ -235,7 +238,7 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     }
     // force_divfree on the nonlinear term; zero mode cleared
     const bool kzero = (a == 0 && l == 0 && ix == 0);
-    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), tt);
+    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)__drcp_rn(k2), tt);
     if (kzero) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) tt[c] = zero_c<T>();
@@ -267,7 +270,7 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
                                   (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 / (T)3)
                           : v0[c];
         // final force_divfree of the state (vorticity_equation.cpp:436)
-        if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), o);
+        if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)__drcp_rn(k2), o);
         if (kzero) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
@@ -400,7 +403,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 cpx<T>* w = &tile[l * PR + WSRC + col * 3];
                 cpx<T> u[3];
                 if (k2 <= kp.kM2 && k2 > 0.0) {
-                    const T ik2 = (T)(1.0 / k2);
+                    const T ik2 = (T)__drcp_rn(k2);
                     cpx<T> wv[3] = {w[0], w[1], w[2]};
                     curl<T>((T)kx, (T)ky, (T)kz, wv, u);
 #pragma unroll
@@ -1050,14 +1053,28 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         __syncthreads();
         if constexpr (WRITE_RU) {
             // real u (u pencils after the inverse transform) in natural x order
-            T* rout = mreal(mem[m], rl.rout);
-            for (int e = tid; e < ROWS * N * 3; e += ROW_THREADS) {
-                const int c = e % 3;
-                const int r2 = e / 3;
-                const int xx = r2 % N;
-                const int r = r2 / N;
-                const cpx<T> z = P[r * RG + c * PL + posn[xx >> 1]];
-                rout[(row0 + r) * (N * 3) + xx * 3 + c] = (xx & 1) ? z.y : z.x;
+            // 16-byte vectors of the (contiguous) output rows
+            T* rout = mreal(mem[m], rl.rout) + row0 * (N * 3);
+            const T* PT = reinterpret_cast<const T*>(P);
+            constexpr int VR = 16 / (int)sizeof(T);
+            constexpr int RV = N * 3 / VR;  // vectors per row
+            for (int v = tid; v < ROWS * RV; v += ROW_THREADS) {
+                const int r = v / RV;
+                const int e0 = (v - r * RV) * VR;
+                T val[VR];
+#pragma unroll
+                for (int i = 0; i < VR; ++i) {
+                    const int e = e0 + i;
+                    const int xx = e / 3;
+                    const int c = e - 3 * xx;
+                    val[i] = PT[2 * (r * RG + c * PL + posn[xx >> 1]) + (xx & 1)];
+                }
+                if constexpr (VR == 4)
+                    *reinterpret_cast<float4*>(rout + r * (N * 3) + e0) =
+                        make_float4(val[0], val[1], val[2], val[3]);
+                else
+                    *reinterpret_cast<double2*>(rout + r * (N * 3) + e0) =
+                        make_double2(val[0], val[1]);
             }
             if constexpr (NS == 2) __syncthreads();  // phase E overwrites the u pencils
         }
@@ -1194,7 +1211,7 @@ __global__ void velocity_kernel(const KParams kp, const cpx<T>* __restrict__ w, 
     if (k2 <= kp.kM2 && k2 > 0.0) {
         cpx<T> wv[3] = {w[pt * 3], w[pt * 3 + 1], w[pt * 3 + 2]};
         curl<T>((T)kx, (T)ky, (T)kz, wv, o);
-        const T ik2 = (T)(1.0 / k2);
+        const T ik2 = (T)__drcp_rn(k2);
 #pragma unroll
         for (int c = 0; c < 3; ++c) o[c] = scale(o[c], ik2);
     } else {
@@ -1222,7 +1239,7 @@ __global__ void lowpass_divfree_kernel(const KParams kp, cpx<T>* a) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) v[c] = zero_c<T>();
     }
-    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)(1.0 / k2), v);
+    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)__drcp_rn(k2), v);
     if (e == 0) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) v[c] = zero_c<T>();

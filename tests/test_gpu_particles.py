@@ -95,3 +95,26 @@ def test_arbitrary_global_indices_come_back_sorted():
     assert rel_err(r, rps.rhs[:, order]) < 1e-12
     ps.close()
     ve.close()
+
+
+@pytest.mark.parametrize("n,nm", [(32, (1, 1)), (32, (3, 2)), (64, (2, 0)), (64, (5, 2))])
+def test_fp32_field_sample_error_bound(n, nm):
+    # Precision form: with an FP32 field the x sums of each stencil row run in
+    # FP32 (weights rounded to FP32), the rest in FP64.  Against the FP64
+    # oracle sampling of the same FP32 field the error stays below 2e-6 of
+    # max|u| (FP32 rounding of 2n+2 weights and partial sums).
+    from bfps_b200.solver import vorticity_equation, particles_system
+    nb, mm = nm
+    ve = vorticity_equation(n, precision="single")
+    ve.set_cvorticity(ic.vorticity_ic(n, seed=5, dtype=np.complex64))
+    ve.velocity_rspace()
+    field = ve.get_rvelocity()[:, :, :n, :].astype(np.float64)
+    pos = ic.tracer_ic(3000, seed=6)
+    pos[:4] = [[0, 0, 0], [2 * np.pi - 1e-9, 0.2, 6.0], [-0.3, 7.0, 13.1], [6.27, 3.0, 0.01]]
+    ps = particles_system(ve, pos, nb, mm, nsteps=2)
+    got = ps.sample_velocity()
+    want = P.sample(field, pos, nb, mm, P.Geometry(n, n, n))
+    err = np.abs(got - want).max() / np.abs(field).max()
+    assert err < 2e-6, err
+    ps.close()
+    ve.close()
