@@ -33,13 +33,13 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # 512^3 FP32 + 4e6 tracers (n=3, m=2), AB3
     "C3": dict(n=512, precision="single", nu=0.002, dt=0.001, k0=4.0, ntracers=4_000_000,
-               neighbours=3, smoothness=2, nsteps_ab=3, dealias=1),
+               neighbours=3, smoothness=2, nsteps_ab=3, dealias=1, accuracy_steps=100),
     # the plain FP64 path at 512^3 (comparator of the precision form)
     "C3_fp64": dict(n=512, precision="double", nu=0.002, dt=0.001, k0=4.0,
                     ntracers=4_000_000, neighbours=3, smoothness=2, nsteps_ab=3, dealias=1),
     # 256^3 FP32 + 1e5 tracers (n=2, m=2), AB4
     "C2": dict(n=256, precision="single", nu=0.005, dt=0.002, k0=3.0, ntracers=100_000,
-               neighbours=2, smoothness=2, nsteps_ab=4, dealias=1),
+               neighbours=2, smoothness=2, nsteps_ab=4, dealias=1, accuracy_steps=200),
     # 32^3 FP64, 1024 tracers, 6-point Lagrange, AB2, 2/3 dealiasing
     "C1": dict(n=32, precision="double", nu=0.1, dt=0.01, k0=3.0, ntracers=1024,
                neighbours=2, smoothness=0, nsteps_ab=2, dealias=0),
@@ -210,6 +210,40 @@ def build_solver(cfg, w0, pos, device):
     return ve, ps
 
 
+def precision_report(cfg, w0, pos, device, nsteps):
+    """Precision form against FP64: the same initial field (the FP32-rounded
+    one) and tracers stepped nsteps times in FP32 and in FP64; relative error
+    of the energy spectrum E(k) = tr(spec_uu)/2 over the shells holding at
+    least 1e-6 of the peak shell energy, of the total energy, of the
+    dissipation eps = 2 nu Omega, and the largest tracer displacement error
+    relative to the box (2 pi)."""
+    from bfps_b200.solver import NSVEparticles_step
+    res = {}
+    for prec in ("single", "double"):
+        c = dict(cfg, precision=prec)
+        w = w0.astype(np.complex64).astype(np.complex128 if prec == "double" else np.complex64)
+        ve, ps = build_solver(c, w, pos, device)
+        NSVEparticles_step(ve, ps, cfg["dt"], nsteps)
+        st = ve.do_stats()
+        sv, sw = st["velocity"][0], st["vorticity"][0]
+        ek = 0.5 * np.einsum("kii->k", sv)
+        omega = 0.5 * np.einsum("kii->k", sw).sum()
+        res[prec] = (ek, 2 * cfg["nu"] * omega, ps.state()[0])
+        ps.close()
+        ve.close()
+    ek32, eps32, p32 = res["single"]
+    ek64, eps64, p64 = res["double"]
+    keep = ek64 >= 1e-6 * ek64.max()
+    rel = np.abs(ek32[keep] - ek64[keep]) / ek64[keep]
+    return {"steps": nsteps, "spectrum_max_rel": float(rel.max()),
+            "spectrum_shells": int(keep.sum()),
+            "energy_rel": float(abs(ek32.sum() - ek64.sum()) / ek64.sum()),
+            "dissipation_rel": float(abs(eps32 - eps64) / eps64),
+            "positions_max_abs_over_box": float(np.abs(p32 - p64).max() / (2 * np.pi)),
+            "how": "same FP32-rounded initial field and tracers, stepped in FP32 and FP64 "
+                   "with this engine; shells with E64(k) >= 1e-6 max"}
+
+
 def run_ours(args, cfg):
     import torch
     from bfps_b200 import _lib
@@ -336,10 +370,12 @@ def run_ours(args, cfg):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(cfg, args.cpu_budget)
     ps.close()
     ve.close()
+    if cfg.get("accuracy_steps") and cfg["precision"] == "single" and not args.no_precision:
+        out["precision_error"] = precision_report(cfg, w0, pos, dev, cfg["accuracy_steps"])
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(cfg, args.cpu_budget)
     if pg is not None:
         pg.destroy_process_group()
     if rank == 0:
@@ -584,10 +620,21 @@ class CpuSample:
         return 3 * stage_s + tracer_s, stage_s, tracer_s
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(cfg, budget):
     smp = CpuSample(cfg, 20_000)
     step_s, stage_s, tracer_s = smp.run()
     return {"value": round(1.0 / step_s, 6), "unit": "steps/s", "cores": smp.cores, "kind": "port",
+            "cpu_model": cpu_model(),
             "sample": ("CPU restatement (numpy + scipy.fft, %d workers): one IF-RK3 stage at "
                        "%d^3 timed (%.2f s, x3) + tracer step for %d of %d tracers (%.2f s "
                        "scaled)" % (smp.cores, cfg["n"], stage_s, smp.nt, cfg["ntracers"],
@@ -626,7 +673,7 @@ def run_reference(args, cfg):
         "config": {"workload": args.workload, "grid": cfg["n"], "tracers": cfg["ntracers"]},
         "impl": "reference",
         "cpu_baseline": {"value": round(1.0 / s, 6), "unit": "steps/s", "cores": smp.cores,
-                         "kind": "port",
+                         "kind": "port", "cpu_model": cpu_model(),
                          "sample": "per step: one IF-RK3 stage at %d^3 (x3) + tracer step for %d "
                                    "of %d tracers (scaled); %d samples timed (warm-up skipped: "
                                    "the CPU path has no warm-up state) within a %d s budget" % (
@@ -644,9 +691,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default="C3", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=120.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the FP32-vs-FP64 error report of the FP32 workloads")
     ap.add_argument("--grid", type=int, default=None,
                     help="override the workload's grid size N (profiling cases)")
     ap.add_argument("--tracers", type=int, default=None,
