@@ -194,14 +194,18 @@ static KParams kparams(const bfg_ctx* c, double dt) {
 // cudaFuncSetAttribute once per kernel and device
 template <typename K>
 static cudaError_t ensure_smem(K kernel, size_t bytes, int device) {
+    // the attribute is a ceiling: only ever raise it (a lower value would
+    // reject later launches that need more), and only past the default
+    if (bytes <= 48 * 1024) return cudaSuccess;
     static std::mutex mu;
-    static std::unordered_map<long long, bool> done;
+    static std::unordered_map<long long, size_t> done;
     const long long key = (long long)(uintptr_t)(void*)kernel * 64 + device;
     std::lock_guard<std::mutex> lk(mu);
-    if (done.count(key)) return cudaSuccess;
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)bytes);
-    if (e == cudaSuccess) done[key] = true;
+    if (e == cudaSuccess) done[key] = bytes;
     return e;
 }
 
