@@ -117,37 +117,46 @@ __device__ __forceinline__ void row_accumulate(const T* __restrict__ row, int x0
     }
 }
 
+// 32-byte vector load (one L1 sector per lane), sm_100; p 32-byte aligned
+__device__ __forceinline__ void ld_v8(const float* p, float* v) {
+    asm volatile("ld.global.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+                   "=f"(v[6]), "=f"(v[7])
+                 : "l"(p));
+}
+
 // FP32 field (precision form): the x sums of each stencil row run in FP32
 // with the x weights rounded to FP32; the y/z weights, the accumulation of
 // the row sums and everything after stay FP64.  Three conversions per row
-// instead of one per value.  A row segment is read as 16-byte vectors from
-// its aligned-down start; instead of shifting the loaded words, the x
-// weights are shifted once per tracer (word i of the aligned block belongs to
-// point (i - off) / 3, component (i - off) mod 3) and the sums are kept per
-// word phase i mod 3, mapped to components at the end.
+// instead of one per value.  A row segment is read as 32-byte vectors (one
+// L1 sector each) from its aligned-down start; instead of shifting the loaded
+// words, the x weights are shifted once per tracer (word i of the aligned
+// block belongs to point (i - off) / 3, component (i - off) mod 3) and the
+// sums are kept per word phase i mod 3, mapped to components at the end.
 template <int NB>
 __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int N, const int* g,
                                                int x0, const double* wx, const double* wy,
                                                const double* wz, double& a0, double& a1,
                                                double& a2) {
     constexpr int NP = 2 * NB + 2;
-    constexpr int NV = (3 * NP + 3) / 4 + 1;  // vectors covering any alignment
-    constexpr int NF = 4 * NV;
+    constexpr int VW = 8;                                // floats per vector
+    constexpr int NV = (3 * NP + 2 * (VW - 1)) / VW;     // vectors covering any alignment
+    constexpr int NF = VW * NV;
     const size_t rowN = (size_t)N;
     float wxf[NP];
 #pragma unroll
     for (int ix = 0; ix < NP; ++ix) wxf[ix] = (float)wx[ix];
     if (x0 >= 0 && x0 + NP <= N) {
         const int e0 = x0 * 3;
-        const int base = e0 & ~3;
+        const int base = e0 & ~(VW - 1);
         const int off = e0 - base;
-        const int maxv = (N * 3 - base) / 4;  // vectors left in the row
+        const int maxv = (N * 3 - base) / VW;  // vectors left in the row
         float wt[NF];
 #pragma unroll
         for (int i = 0; i < NF; ++i) {
             float w = 0.f;
 #pragma unroll
-            for (int o = 0; o < 4; ++o) {
+            for (int o = 0; o < VW; ++o) {
                 const int k = i - o;
                 if (k >= 0 && k < 3 * NP) w = (off == o) ? wxf[k / 3] : w;
             }
@@ -165,11 +174,11 @@ __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
                     if (v < maxv) {
-                        const float4 q = *reinterpret_cast<const float4*>(row + 4 * v);
-                        sp[(4 * v + 0) % 3] = fmaf(q.x, wt[4 * v + 0], sp[(4 * v + 0) % 3]);
-                        sp[(4 * v + 1) % 3] = fmaf(q.y, wt[4 * v + 1], sp[(4 * v + 1) % 3]);
-                        sp[(4 * v + 2) % 3] = fmaf(q.z, wt[4 * v + 2], sp[(4 * v + 2) % 3]);
-                        sp[(4 * v + 3) % 3] = fmaf(q.w, wt[4 * v + 3], sp[(4 * v + 3) % 3]);
+                        float q[VW];
+                        ld_v8(row + VW * v, q);
+#pragma unroll
+                        for (int u = 0; u < VW; ++u)
+                            sp[(VW * v + u) % 3] = fmaf(q[u], wt[VW * v + u], sp[(VW * v + u) % 3]);
                     }
                 }
                 const double bzy = wz[iz] * wy[iy];
