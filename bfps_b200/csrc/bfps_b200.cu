@@ -229,13 +229,13 @@ struct Engine {
         const int ntx = (N / 2 + 1 + TKX - 1) / TKX;
         const int tiles_per = ntx * N;
         const int ntiles = tiles_per * nmem;
-        const int grid = std::min(ntiles, c->nsm);
+        const int grid = std::min(ntiles, c->nsm * col_ctas<T, N, MODE>());
         constexpr int kind = (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) ? K_IZ
                              : (MODE == CM_Y_INV1 || MODE == CM_Y_INV2)                  ? K_IY
                              : (MODE == CM_Y_FWD1)                                      ? K_FY
                                                                                         : K_FZ;
         Prof pr(c, kind);
-        kern<<<grid, COL_THREADS, smem, c->stream>>>(mem, rl, (const C*)c->tw, ntx, tiles_per,
+        kern<<<grid, col_threads<T, N, MODE>(), smem, c->stream>>>(mem, rl, (const C*)c->tw, ntx, tiles_per,
                                                      ntiles);
         return after_launch(c, "col_pass");
     }
@@ -252,9 +252,9 @@ struct Engine {
             CU(ensure_smem(kern, smem, c->device));
             const int tiles_per = N * N / ROWS;
             const int ntiles = tiles_per * nmem;
-            const int grid = std::min(ntiles, c->nsm);
+            const int grid = std::min(ntiles, c->nsm * rnl_ctas<T, N>());
             Prof pr(c, K_X);
-            kern<<<grid, ROW_THREADS, smem, c->stream>>>(mem, rl, (const C*)c->tw, tiles_per,
+            kern<<<grid, rnl_threads<T, N>(), smem, c->stream>>>(mem, rl, (const C*)c->tw, tiles_per,
                                                          ntiles);
             return after_launch(c, "row_nonlin");
         }

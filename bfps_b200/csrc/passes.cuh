@@ -95,8 +95,8 @@ __host__ __device__ constexpr bool col_inverse(int mode) {
 __host__ __device__ constexpr int pow2floor(int v) {
     return v < 2 ? 1 : 2 * pow2floor(v / 2);
 }
-constexpr int COL_THREADS = 512;
-constexpr int SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per CTA we plan for
+constexpr int SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per SM we plan for
+__host__ __device__ constexpr bool col_fz(int mode) { return mode >= 5 && mode <= 7; }
 
 // tile row pitch (complex) for a tile of TKX kx columns: keeps every row
 // 16-byte aligned and breaks the worst bank patterns
@@ -108,22 +108,41 @@ __host__ __device__ constexpr int col_pitch_for(int tkx) {
 __host__ __device__ constexpr int col_nrk(int mode) {
     return mode == CM_FZ_RK1 ? 1 : ((mode == CM_FZ_RK2 || mode == CM_FZ_RK3) ? 2 : 0);
 }
-// two tile buffers + the RK operand tile + twiddles
+// Launch shape of a column pass.  The IZ passes (which read half of what
+// they write) run two 256-thread CTAs per SM with one tile buffer each, where
+// such a tile still has rows of at least 96 bytes: one CTA's barrier waits
+// and loads are covered by the other CTA's work (measured faster for IZ,
+// slower for IY and FY).  Otherwise one 512-thread CTA per SM with two tile
+// buffers, the next tile loading while this one is transformed.
+// shared memory: nbuf tile buffers + the RK operand tile + twiddles
 template <typename T, int N, int MODE>
-__host__ __device__ constexpr size_t col_bytes_for(int tkx) {
-    return (size_t)(2 * N * col_pitch_for<T, col_nb(MODE)>(tkx) + col_nrk(MODE) * N * 3 * tkx + N) *
+__host__ __device__ constexpr size_t col_bytes_nb(int tkx, int nbuf) {
+    return (size_t)(nbuf * N * col_pitch_for<T, col_nb(MODE)>(tkx) + col_nrk(MODE) * N * 3 * tkx +
+                    N) *
            sizeof(cpx<T>);
 }
-// kx columns per tile: the widest power of two (<= 16) that fits the budget
+// kx columns per tile: the widest power of two (<= 16) within the budget
 template <typename T, int N, int MODE>
-__host__ __device__ constexpr int col_tkx_from(int tkx) {
-    return (tkx <= 1 || col_bytes_for<T, N, MODE>(tkx) <= (size_t)SMEM_BUDGET)
+__host__ __device__ constexpr int col_tkx_fit(int tkx, int nbuf, size_t budget) {
+    return (tkx <= 1 || col_bytes_nb<T, N, MODE>(tkx, nbuf) <= budget)
                ? tkx
-               : col_tkx_from<T, N, MODE>(tkx / 2);
+               : col_tkx_fit<T, N, MODE>(tkx / 2, nbuf, budget);
 }
 template <typename T, int N, int MODE>
+__host__ __device__ constexpr bool col_two() {
+    return (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) &&
+           col_tkx_fit<T, N, MODE>(16, 1, SMEM_BUDGET / 2) * 3 * (int)sizeof(cpx<T>) >= 96;
+}
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr int col_threads() { return col_two<T, N, MODE>() ? 256 : 512; }
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr int col_ctas() { return col_two<T, N, MODE>() ? 2 : 1; }
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr int col_nbuf() { return col_two<T, N, MODE>() ? 1 : 2; }
+template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_tkx() {
-    return col_tkx_from<T, N, MODE>(16);
+    return col_two<T, N, MODE>() ? col_tkx_fit<T, N, MODE>(16, 1, SMEM_BUDGET / 2)
+                                 : col_tkx_fit<T, N, MODE>(16, 2, SMEM_BUDGET);
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_pitch() {
@@ -131,7 +150,7 @@ __host__ __device__ constexpr int col_pitch() {
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t col_smem_bytes() {
-    return col_bytes_for<T, N, MODE>(col_tkx<T, N, MODE>());
+    return col_bytes_nb<T, N, MODE>(col_tkx<T, N, MODE>(), col_nbuf<T, N, MODE>());
 }
 
 template <int N>
@@ -293,7 +312,7 @@ __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
     constexpr int VPE = VB / (int)sizeof(cpx<T>) > 0 ? VB / (int)sizeof(cpx<T>) : 1;  // complex per copy
     constexpr int WV = W / VPE;
     const int nvalid = (3 * ncol + VPE - 1) / VPE;
-    for (int e = tid; e < N * NBIN * WV; e += COL_THREADS) {
+    for (int e = tid; e < N * NBIN * WV; e += col_threads<T, N, MODE>()) {
         const int v = e % WV;
         const int r = e / WV;
         const int b = r % NBIN;
@@ -307,9 +326,11 @@ __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
 }
 
 template <typename T, int N, int MODE>
-__global__ void __launch_bounds__(COL_THREADS, 1)
+__global__ void __launch_bounds__(col_threads<T, N, MODE>(), col_ctas<T, N, MODE>())
 col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
          int ntx, int tiles_per, int ntiles) {
+    constexpr int NT = col_threads<T, N, MODE>();
+    constexpr int NBUF = col_nbuf<T, N, MODE>();
     constexpr int NB = col_nb(MODE);
     constexpr int TKX = col_tkx<T, N, MODE>();
     constexpr int W = 3 * TKX;                     // complex per row per buffer
@@ -323,13 +344,13 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     constexpr int NRK = col_nrk(MODE);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* bufs = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* rkt = bufs + 2 * TILE;        // RK operand tile [arr][l][W] (FZ passes)
+    cpx<T>* rkt = bufs + NBUF * TILE;     // RK operand tile [arr][l][W] (FZ passes)
     cpx<T>* tw = rkt + NRK * N * W;
 
     constexpr int NXV = N / 2 + 1;
     constexpr size_t nxp3 = (size_t)(N / 2 + 4) * 3;
     const int tid = threadIdx.x;
-    for (int i = tid; i < N; i += COL_THREADS) tw[i] = tw_g[i];
+    for (int i = tid; i < N; i += NT) tw[i] = tw_g[i];
 
     // tile t: member t / tiles_per, then (a, kx-tile) with the kx-tile fastest
     int t = blockIdx.x;
@@ -342,14 +363,14 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     cp_async_commit();
     __shared__ Member<T> mb;  // this tile's member, read once per tile
     for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
-        cpx<T>* tile = bufs + (it & 1) * TILE;
+        cpx<T>* tile = bufs + (NBUF == 2 ? (it & 1) * TILE : 0);
         const int m = t / tiles_per, tl = t - m * tiles_per;
         {
             // the previous tile ended with a barrier: nobody reads mb now
             constexpr int NWORDS = (int)(sizeof(Member<T>) / sizeof(int));
             const int* src = reinterpret_cast<const int*>(&mem[m]);
             int* dst = reinterpret_cast<int*>(&mb);
-            for (int i = tid; i < NWORDS; i += COL_THREADS) dst[i] = src[i];
+            for (int i = tid; i < NWORDS; i += NT) dst[i] = src[i];
         }
         if constexpr (NRK > 0) {
             // RK operands of this tile: rows S[ky=a][kz=l], streamed while the
@@ -359,7 +380,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             const cpx<T>* rk_v0 = mbuf(mem[m], rl.v0);  // mb is not yet visible to all
             const cpx<T>* rk_vp = mbuf(mem[m], rl.vp);
             const int nvalid = (3 * min(TKX, NXV - kx0) + VPE - 1) / VPE;
-            for (int e = tid; e < N * NRK * WV; e += COL_THREADS) {
+            for (int e = tid; e < N * NRK * WV; e += NT) {
                 const int v = e % WV;
                 const int r = e / WV;
                 const int arr = r % NRK;
@@ -371,7 +392,8 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             }
             cp_async_commit();
         }
-        {
+        if constexpr (NBUF == 2) {
+            // the next tile streams into the other buffer while this one is transformed
             const int tn = t + gridDim.x;
             if (tn < ntiles) {
                 const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
@@ -383,7 +405,8 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             cp_async_commit();
         }
         if constexpr (NRK > 0) cp_async_wait<2>();
-        else cp_async_wait<1>();
+        else if constexpr (NBUF == 2) cp_async_wait<1>();
+        else cp_async_wait<0>();
         __syncthreads();
         const int a = tl / ntx;
         const int kx0 = (tl % ntx) * TKX;
@@ -394,7 +417,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         if constexpr (MODE == CM_IZ_VEL || MODE == CM_IZ_U) {
             constexpr int WSRC = (MODE == CM_IZ_VEL) ? W : 0;  // slot holding w^
             const double ky = kwrap<N>(a, kp.dky);
-            for (int e = tid; e < N * TKX; e += COL_THREADS) {
+            for (int e = tid; e < N * TKX; e += NT) {
                 const int col = e % TKX;
                 const int l = e / TKX;
                 const double kz = kwrap<N>(l, kp.dkz);
@@ -423,12 +446,12 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         constexpr int P = NB * W;
         constexpr int NST = plan_nstages(N);
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
-            dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, COL_THREADS);
+            dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, NT);
             cp_async_wait<1>();  // RK operand tile of this tile
             __syncthreads();
             // ---- epilogue: one thread per mode (kz = l, kx = kx0 + col)
             const double ky = kwrap<N>(a, kp.dky);
-            for (int e = tid; e < N * TKX; e += COL_THREADS) {
+            for (int e = tid; e < N * TKX; e += NT) {
                 const int col = e % TKX;
                 const int l = e / TKX;
                 if (col >= ncol) continue;
@@ -439,14 +462,14 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                                      mb.fac, mbuf(mb, rl.fsrc), mbuf(mb, rl.out0));
             }
         } else {
-            dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, COL_THREADS);
+            dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, NT);
             // last stage fused with the store: block b of R positions holds
             // frequencies f(b) + (N/R) q; lanes take consecutive pencils, i.e.
             // consecutive complex numbers of one output row chunk
             constexpr int R = plan_radix(N, NST - 1);
             constexpr int NW = P * (N / R);
             const int nval = 3 * ncol;
-            for (int w = tid; w < NW; w += COL_THREADS) {
+            for (int w = tid; w < NW; w += NT) {
                 const int pp = w % P;
                 const int bb = w / P;
                 cpx<T> v[R];
@@ -462,7 +485,17 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                     dst[col_out_row<N, MODE>(a, f0 + (N / R) * m) * nxp3] = v[m];
             }
         }
-        __syncthreads();  // this buffer is refilled by the load issued next iteration
+        __syncthreads();  // this buffer is refilled by the next load
+        if constexpr (NBUF == 1) {
+            const int tn = t + gridDim.x;
+            if (tn < ntiles) {
+                const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
+                const int kx0n = (tln % ntx) * TKX;
+                col_issue_load<T, N, MODE>(bufs, mbuf(mem[mn], rl.in0), mbuf(mem[mn], rl.in1),
+                                           tln / ntx, kx0n, min(TKX, NXV - kx0n), nxp3, tid);
+            }
+            cp_async_commit();
+        }
     }
     cp_async_wait<0>();
 }
@@ -780,11 +813,25 @@ __host__ __device__ constexpr size_t rnl_bytes_for(int R) {
                sizeof(cpx<T>) +
            (size_t)(N / 2) * 4;
 }
+// rows per tile within a shared-memory budget
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_rows_fit(int R, size_t budget) {
+    return (R <= 1 || (rnl_bytes_for<T, N>(R) <= budget && R <= (N * N) / 296))
+               ? (R < 1 ? 1 : R)
+               : rnl_rows_fit<T, N>(R / 2, budget);
+}
+// CTAs per SM of the fused row pass: two 256-thread CTAs where each still
+// holds at least 4 rows (slightly faster: one CTA's barriers are covered by
+// the other), else one 512-thread CTA
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_ctas() {
+    return rnl_rows_fit<T, N>(16, SMEM_BUDGET / 2 - 2048) >= 4 ? 2 : 1;
+}
+template <typename T, int N>
+__host__ __device__ constexpr int rnl_threads() { return 512 / rnl_ctas<T, N>(); }
 template <typename T, int N>
 __host__ __device__ constexpr int rnl_rows_from(int R) {
-    return (R <= 1 || (rnl_bytes_for<T, N>(R) <= (size_t)ROW_BUDGET && R <= (N * N) / 296))
-               ? (R < 1 ? 1 : R)
-               : rnl_rows_from<T, N>(R / 2);
+    return rnl_rows_fit<T, N>(R, SMEM_BUDGET / rnl_ctas<T, N>() - 2048);
 }
 template <typename T, int N>
 __host__ __device__ constexpr int rnl_rows() { return rnl_rows_from<T, N>(16); }
@@ -849,9 +896,10 @@ __device__ __forceinline__ cpx<T> r2c_hi(cpx<T> zk, cpx<T> zm, cpx<T> w) {
 }
 
 template <typename T, int N, bool WRITE_RU>
-__global__ void __launch_bounds__(ROW_THREADS, 1)
+__global__ void __launch_bounds__(rnl_threads<T, N>(), rnl_ctas<T, N>())
 row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
            int tiles_per, int ntiles) {
+    constexpr int RNL_THREADS = rnl_threads<T, N>();
     constexpr int M = N / 2;
     constexpr int NS = plan_nstages(M);
     constexpr int R0 = plan_radix(M, 0);
@@ -881,19 +929,19 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
     int* posn = reinterpret_cast<int*>(tw0 + rnl_tw0<N>());
     const int tid = threadIdx.x;
 
-    for (int i = tid; i < N; i += ROW_THREADS) tw[i] = tw_g[i];
-    for (int i = tid; i < rnl_tw0<N>(); i += ROW_THREADS) {
+    for (int i = tid; i < N; i += RNL_THREADS) tw[i] = tw_g[i];
+    for (int i = tid; i < rnl_tw0<N>(); i += RNL_THREADS) {
         const int j = i / (R0 - 1), q = i - j * (R0 - 1) + 1;
         tw0[i] = tw_g[2 * j * q];
     }
     if constexpr (WRITE_RU)
-        for (int i = tid; i < M; i += ROW_THREADS) posn[i] = dif_position<M>(i);
+        for (int i = tid; i < M; i += RNL_THREADS) posn[i] = dif_position<M>(i);
 
     auto issue = [&](int tt) {
         const int mm = tt / tiles_per, tl = tt - mm * tiles_per;
         const cpx<T>* su = mbuf(mem[mm], rl.in0) + (size_t)tl * ROWS * RL;
         const cpx<T>* sw = mbuf(mem[mm], rl.in1) + (size_t)tl * ROWS * RL;
-        for (int e = tid; e < 2 * NV; e += ROW_THREADS) {
+        for (int e = tid; e < 2 * NV; e += RNL_THREADS) {
             const int b = e >= NV ? 1 : 0;
             const int v = e - b * NV;
             cp_async16(&st[b * ROWS * RL + v * VPE], &(b ? sw : su)[v * VPE]);
@@ -909,7 +957,7 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         const size_t row0 = (size_t)tl * ROWS;
 
         // A: C2R pre-processing + DIF stage 0, staging rows -> pencils
-        for (int e = tid; e < 6 * ROWS * H0; e += ROW_THREADS) {
+        for (int e = tid; e < 6 * ROWS * H0; e += RNL_THREADS) {
             const int u = e % H0;
             const int p = e / H0;  // = r * 6 + c6
             const int r = p / 6, c6 = p - 6 * r;
@@ -975,16 +1023,16 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         cp_async_commit();
 
         // B: middle DIF stages over the six pencils of each row
-        dif_range<T, M, 1, NS - 1, true, 6 * ROWS, L6, 2, N>(P, tw, tid, ROW_THREADS);
+        dif_range<T, M, 1, NS - 1, true, 6 * ROWS, L6, 2, N>(P, tw, tid, RNL_THREADS);
         if constexpr (SPLIT) {
-            dif_stage<T, M, NS - 1, true, 3 * ROWS, LW, 2, N>(P, tw, tid, ROW_THREADS);
+            dif_stage<T, M, NS - 1, true, 3 * ROWS, LW, 2, N>(P, tw, tid, RNL_THREADS);
             __syncthreads();
         }
 
         // C: last DIF stage, u x w / N^3, first DIT stage (product -> w pencils)
         {
             const T inv_np = (T)1 / ((T)N * (T)N * (T)N);
-            for (int e = tid; e < ROWS * NBZ; e += ROW_THREADS) {
+            for (int e = tid; e < ROWS * NBZ; e += RNL_THREADS) {
                 const int rlo = e % G;
                 const int t2 = e / G;
                 const int bb = t2 % NBZ;
@@ -1058,7 +1106,7 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
             const T* PT = reinterpret_cast<const T*>(P);
             constexpr int VR = 16 / (int)sizeof(T);
             constexpr int RV = N * 3 / VR;  // vectors per row
-            for (int v = tid; v < ROWS * RV; v += ROW_THREADS) {
+            for (int v = tid; v < ROWS * RV; v += RNL_THREADS) {
                 const int r = v / RV;
                 const int e0 = (v - r * RV) * VR;
                 T val[VR];
@@ -1080,10 +1128,10 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         }
 
         // D: middle DIT stages over the w pencils
-        dit_range<T, M, NS - 2, 1, false, 3 * ROWS, LW, 2, N>(P, tw, tid, ROW_THREADS);
+        dit_range<T, M, NS - 2, 1, false, 3 * ROWS, LW, 2, N>(P, tw, tid, RNL_THREADS);
 
         // E: DIT stage 0 + R2C post-processing, w pencils -> output rows
-        for (int e = tid; e < 3 * ROWS * H0; e += ROW_THREADS) {
+        for (int e = tid; e < 3 * ROWS * H0; e += RNL_THREADS) {
             const int u = e % H0;
             const int p = e / H0;  // = r * 3 + c
             const int r = p / 3, c = p - 3 * r;
@@ -1133,7 +1181,7 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
             }
         }
         // padding points of the output rows carry zeros
-        for (int i = tid; i < ROWS * (RL - 3 * (M + 1)); i += ROW_THREADS) {
+        for (int i = tid; i < ROWS * (RL - 3 * (M + 1)); i += RNL_THREADS) {
             const int r = i / (RL - 3 * (M + 1));
             P[r * RG + 3 * (M + 1) + (i - r * (RL - 3 * (M + 1)))] = zero_c<T>();
         }
@@ -1142,7 +1190,7 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         {
             cpx<T>* wout = mbuf(mem[m], rl.out0) + row0 * RL;
             float4* dst = reinterpret_cast<float4*>(wout);
-            for (int v = tid; v < NV; v += ROW_THREADS) {
+            for (int v = tid; v < NV; v += RNL_THREADS) {
                 const int r = v / (RL / VPE);
                 const cpx<T>* s = P + r * RG + (v - r * (RL / VPE)) * VPE;
                 float4 val;
