@@ -128,10 +128,18 @@ __host__ __device__ constexpr int col_tkx_fit(int tkx, int nbuf, size_t budget) 
                ? tkx
                : col_tkx_fit<T, N, MODE>(tkx / 2, nbuf, budget);
 }
+// one tile over all N/2+1 kx columns where it fits (small grids): otherwise
+// the Nyquist column kx = N/2 gets a tile of its own, which costs a full tile
+template <typename T, int N, int MODE>
+__host__ __device__ constexpr int col_tkx_sel(int nbuf, size_t budget) {
+    return col_bytes_nb<T, N, MODE>(N / 2 + 1, nbuf) <= budget
+               ? N / 2 + 1
+               : col_tkx_fit<T, N, MODE>(16, nbuf, budget);
+}
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr bool col_two() {
     return (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) &&
-           col_tkx_fit<T, N, MODE>(16, 1, SMEM_BUDGET / 2) * 3 * (int)sizeof(cpx<T>) >= 96;
+           col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / 2) * 3 * (int)sizeof(cpx<T>) >= 96;
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_threads() { return col_two<T, N, MODE>() ? 256 : 512; }
@@ -141,8 +149,8 @@ template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_nbuf() { return col_two<T, N, MODE>() ? 1 : 2; }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_tkx() {
-    return col_two<T, N, MODE>() ? col_tkx_fit<T, N, MODE>(16, 1, SMEM_BUDGET / 2)
-                                 : col_tkx_fit<T, N, MODE>(16, 2, SMEM_BUDGET);
+    return col_two<T, N, MODE>() ? col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / 2)
+                                 : col_tkx_sel<T, N, MODE>(2, SMEM_BUDGET);
 }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_pitch() {
@@ -325,6 +333,40 @@ __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
     }
 }
 
+// Last FFT stage of a column pass fused with the store: block b of R
+// positions holds frequencies f(b) + (N/R) q; lanes take consecutive pencils,
+// i.e. consecutive complex numbers of one output row chunk.  NYQ: the tile
+// holds the Nyquist column only and PP counts its pencils (3 per buffer).
+template <typename T, int N, int MODE, int PP, bool NYQ>
+__device__ __forceinline__ void col_last_store(const cpx<T>* tile, int tid, const Member<T>& mb,
+                                               const Roles& rl, int a, int kx0, int ncol) {
+    constexpr int NT = col_threads<T, N, MODE>();
+    constexpr int TKX = col_tkx<T, N, MODE>();
+    constexpr int W = 3 * TKX;
+    constexpr int PR = col_pitch<T, N, MODE>();
+    constexpr bool INV = col_inverse(MODE);
+    constexpr int NST = plan_nstages(N);
+    constexpr int R = plan_radix(N, NST - 1);
+    constexpr int NW = PP * (N / R);
+    constexpr size_t nxp3 = (size_t)(N / 2 + 4) * 3;
+    const int nval = 3 * ncol;
+    for (int w = tid; w < NW; w += NT) {
+        const int pn = w % PP;
+        const int bb = w / PP;
+        const int pp = NYQ ? (pn / 3) * W + pn % 3 : pn;
+        cpx<T> v[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) v[m] = tile[pp + (bb * R + m) * PR];
+        dft<T, INV, R>(v);
+        const int bufi = pp / W, q = pp % W;
+        if (q >= nval) continue;
+        cpx<T>* dst = mbuf(mb, (bufi == 0) ? rl.out0 : rl.out1) + (size_t)kx0 * 3 + q;
+        const int f0 = dif_frequency<N>(bb * R);
+#pragma unroll
+        for (int m = 0; m < R; ++m) dst[col_out_row<N, MODE>(a, f0 + (N / R) * m) * nxp3] = v[m];
+    }
+}
+
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(col_threads<T, N, MODE>(), col_ctas<T, N, MODE>())
 col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
@@ -420,6 +462,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             for (int e = tid; e < N * TKX; e += NT) {
                 const int col = e % TKX;
                 const int l = e / TKX;
+                if (col >= ncol) continue;
                 const double kz = kwrap<N>(l, kp.dkz);
                 const double kx = (double)(kx0 + col) * kp.dkx;
                 const double k2 = (kx * kx + ky * ky) + kz * kz;
@@ -444,9 +487,13 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         // ---- FFT along l: NB*W pencils, pencil stride 1, element stride PR --
         using LY = Lay<1, 1, 0, PR>;
         constexpr int P = NB * W;
+        // the tile holding only the Nyquist column transforms just its pencils
+        using LYN = Lay<3, W, 1, PR>;
+        constexpr int PN = NB * 3;
         constexpr int NST = plan_nstages(N);
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
-            dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, NT);
+            if (ncol == TKX) dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, NT);
+            else dif<T, N, INV, PN, LYN, 1, N>(tile, tw, tid, NT);
             cp_async_wait<1>();  // RK operand tile of this tile
             __syncthreads();
             // ---- epilogue: one thread per mode (kz = l, kx = kx0 + col)
@@ -462,27 +509,12 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                                      mb.fac, mbuf(mb, rl.fsrc), mbuf(mb, rl.out0));
             }
         } else {
-            dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, NT);
-            // last stage fused with the store: block b of R positions holds
-            // frequencies f(b) + (N/R) q; lanes take consecutive pencils, i.e.
-            // consecutive complex numbers of one output row chunk
-            constexpr int R = plan_radix(N, NST - 1);
-            constexpr int NW = P * (N / R);
-            const int nval = 3 * ncol;
-            for (int w = tid; w < NW; w += NT) {
-                const int pp = w % P;
-                const int bb = w / P;
-                cpx<T> v[R];
-#pragma unroll
-                for (int m = 0; m < R; ++m) v[m] = tile[pp + (bb * R + m) * PR];
-                dft<T, INV, R>(v);
-                const int bufi = pp / W, q = pp % W;
-                if (q >= nval) continue;
-                cpx<T>* dst = mbuf(mb, (bufi == 0) ? rl.out0 : rl.out1) + (size_t)kx0 * 3 + q;
-                const int f0 = dif_frequency<N>(bb * R);
-#pragma unroll
-                for (int m = 0; m < R; ++m)
-                    dst[col_out_row<N, MODE>(a, f0 + (N / R) * m) * nxp3] = v[m];
+            if (ncol == TKX) {
+                dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, NT);
+                col_last_store<T, N, MODE, P, false>(tile, tid, mb, rl, a, kx0, ncol);
+            } else {
+                dif_range<T, N, 0, NST - 1, INV, PN, LYN, 1, N>(tile, tw, tid, NT);
+                col_last_store<T, N, MODE, PN, true>(tile, tid, mb, rl, a, kx0, ncol);
             }
         }
         __syncthreads();  // this buffer is refilled by the next load
@@ -813,10 +845,15 @@ __host__ __device__ constexpr size_t rnl_bytes_for(int R) {
                sizeof(cpx<T>) +
            (size_t)(N / 2) * 4;
 }
+// at most N^2/296 rows per tile (a single instance then still has a tile for
+// each of two CTAs on every SM), but up to 16 on small grids, whose passes
+// are launched over many instances at once and pay per-tile overheads
+template <int N>
+__host__ __device__ constexpr int rnl_row_cap() { return (N * N) / 296 > 16 ? (N * N) / 296 : 16; }
 // rows per tile within a shared-memory budget
 template <typename T, int N>
 __host__ __device__ constexpr int rnl_rows_fit(int R, size_t budget) {
-    return (R <= 1 || (rnl_bytes_for<T, N>(R) <= budget && R <= (N * N) / 296))
+    return (R <= 1 || (rnl_bytes_for<T, N>(R) <= budget && R <= rnl_row_cap<N>()))
                ? (R < 1 ? 1 : R)
                : rnl_rows_fit<T, N>(R / 2, budget);
 }
