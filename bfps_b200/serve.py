@@ -3,11 +3,13 @@
 A request asks for one DNS solve: grid size N, viscosity, seed, number of
 steps and tracers.  Requests are admitted while their device memory fits an
 HBM budget; admitted requests become ensemble members (their state stays
-resident on the GPU) and advance together, one ensemble step per tick, with
-the stages of all resident requests of the same size batched into one launch
-per pass.  A request that reaches its step count is read back and retired,
-freeing its memory for waiting requests.  Requests that arrive while others
-are running join at the next tick.
+resident on the GPU) and advance together, with the stages of all resident
+requests of the same size batched into one launch per pass.  A tick runs the
+ensemble up to the next event (a resident request reaching its step count,
+or the next arrival as estimated from the measured step time) and
+synchronises once.  A request that reaches its step count is read back and
+retired, freeing its memory for waiting requests.  Requests that arrive
+while others are running join at the next tick.
 
 Nothing here computes on the host: every step is bfg_ens_step.
 """
@@ -91,10 +93,12 @@ def prepare(req):
 
 
 class Server:
-    def __init__(self, hbm_budget=150e9, device=0, use_graphs=False):
+    def __init__(self, hbm_budget=150e9, device=0, use_graphs=False, max_tick=64):
         self.budget = hbm_budget
         self.used = 0
         self.device = device
+        self.max_tick = max_tick   # most ensemble steps between two synchronisations
+        self.step_ms = 0.0         # device time of one ensemble step, last tick
         self.ens = ensemble(device)
         self.ens.use_graphs(use_graphs)
         self.running = {}   # rid -> (request, fs, ps, steps_done)
@@ -156,12 +160,18 @@ class Server:
                 if qi < len(pending):
                     time.sleep(max(0.0, min(0.01, pending[qi].arrival - (clock() - t0))))
                 continue
-            # one ensemble step for every resident request; waiting for it keeps
-            # the host from queueing far ahead of newly admitted requests
-            self.ens.step(1)
-            self.ens.last_ms()
+            # one tick: ensemble steps up to the next event -- the first resident
+            # request reaching its step count, or (by the measured step time)
+            # the next arrival -- then one synchronisation
+            k = min(r[0].steps - r[3] for r in self.running.values())
+            if qi < len(pending) and self.step_ms > 0.0:
+                until = pending[qi].arrival - (clock() - t0)
+                k = min(k, max(1, int(until * 1e3 / self.step_ms)))
+            k = max(1, min(k, self.max_tick))
+            self.ens.step(k)
+            self.step_ms = self.ens.last_ms() / k
             for rid in list(self.running):
-                self.running[rid][3] += 1
+                self.running[rid][3] += k
                 if self.running[rid][3] >= self.running[rid][0].steps:
                     self._finish(rid, clock() - t0)
         return self.done
