@@ -56,6 +56,7 @@ struct bfg_ctx {
     void* dmember = nullptr;   // this context as a one-element Member<T> array
     std::vector<unsigned char> hmember;  // last uploaded copy
     void* stats_ws = nullptr;  // statistics partial sums
+    int* tctr = nullptr;       // tile counters of the persistent passes (self-resetting)
     size_t stats_ws_bytes = 0;
     size_t field_bytes = 0;
     cudaStream_t stream = nullptr;
@@ -235,8 +236,11 @@ struct Engine {
                              : (MODE == CM_Y_FWD1)                                      ? K_FY
                                                                                         : K_FZ;
         Prof pr(c, kind);
+        // dynamic tile order for the IZ passes with at least 8 tiles per CTA
+        constexpr bool iz = MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U;
+        int* tctr = (iz && ntiles >= 8 * grid) ? c->tctr : nullptr;
         kern<<<grid, col_threads<T, N, MODE>(), smem, c->stream>>>(mem, rl, (const C*)c->tw, ntx, tiles_per,
-                                                     ntiles);
+                                                     ntiles, tctr);
         return after_launch(c, "col_pass");
     }
 
@@ -693,7 +697,7 @@ void bfg_ctx_destroy(bfg_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* bufs[] = {c->w0, c->v1, c->v2, c->wa, c->wb, c->ru, c->tw, c->filt, c->fac, c->stats_ws,
-                    c->dmember};
+                    c->dmember, c->tctr};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
@@ -777,6 +781,8 @@ int bfg_ctx_create(bfg_ctx** out, int nx, int ny, int nz, double dkx, double dky
         if (cudaMemset(*b, 0, c->field_bytes) != cudaSuccess) return bail(BFG_ECUDA);
     }
     if (cudaMalloc(&c->tw, (size_t)nx * cb) != cudaSuccess) return bail(BFG_ENOMEM);
+    if (cudaMalloc(&c->tctr, 64) != cudaSuccess || cudaMemset(c->tctr, 0, 64) != cudaSuccess)
+        return bail(BFG_ENOMEM);
     if (cudaMalloc(&c->fac, 3 * (size_t)(c->nxv + 2 * nx) * real_bytes) != cudaSuccess)
         return bail(BFG_ENOMEM);
     if ((rc = upload_tables(c))) return bail(rc);
@@ -1428,6 +1434,7 @@ struct bfg_ens {
     int64_t nbatched = 0;
     bool dirty = true;
     bool use_graphs = true;
+    int* tctr = nullptr;  // tile counters of the launches on this stream
     std::string err;
 };
 
@@ -1545,6 +1552,7 @@ static int ens_prepare(bfg_ens* e) {
         g->launcher.device = c0->device;
         g->launcher.tw = c0->tw;
         g->launcher.stream = e->stream;
+        g->launcher.tctr = e->tctr;
         for (int i : g->members) g->any_tracers = g->any_tracers || e->entries[i].tracers != nullptr;
         // member descriptors
         std::vector<unsigned char> host;
@@ -1642,6 +1650,12 @@ int bfg_ens_create(bfg_ens** out, int device) {
     cudaEventCreate(&e->ev0);
     cudaEventCreate(&e->ev1);
     cudaEventCreateWithFlags(&e->ev_ru, cudaEventDisableTiming);
+    if (cudaMalloc(&e->tctr, 64) != cudaSuccess || cudaMemset(e->tctr, 0, 64) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamDestroy(e->stream);
+        delete e;
+        return BFG_ENOMEM;
+    }
     *out = e;
     return 0;
 }
@@ -1656,6 +1670,7 @@ void bfg_ens_destroy(bfg_ens* e) {
     cudaEventDestroy(e->ev1);
     cudaEventDestroy(e->ev_ru);
     cudaStreamDestroy(e->stream);
+    if (e->tctr) cudaFree(e->tctr);
     delete e;
 }
 

@@ -290,11 +290,12 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
                                   (3 * v0[c].y * f0 + (vp[c].y + dt * tt[c].y) * f1) * (T)0.25)
                           : zero_c<T>();
     } else {
+        const T third = (T)(1.0 / 3.0);  // the division by 3 as a product (within one rounding)
         const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-            o[c] = inside ? mk<T>((v0[c].x * f0 + 2 * (vp[c].x + dt * tt[c].x)) * f0 / (T)3,
-                                  (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 / (T)3)
+            o[c] = inside ? mk<T>((v0[c].x * f0 + 2 * (vp[c].x + dt * tt[c].x)) * f0 * third,
+                                  (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 * third)
                           : v0[c];
         // final force_divfree of the state (vorticity_equation.cpp:436)
         if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)__drcp_rn(k2), o);
@@ -330,6 +331,29 @@ __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
                             (size_t)kx0 * 3 + v * VPE;
         const int bdst = (MODE == CM_IZ_VEL) ? 1 : b;  // w^ goes to slot 1
         cp_async<VB>(&tile[l * PR + bdst * W + v * VPE], src);
+    }
+}
+
+// Dynamic tile scheduling: CTAs take tile numbers from a counter in global
+// memory (tctr[0]), so an SM that runs slower takes fewer tiles instead of
+// holding up the end of the pass (measured faster for the IZ passes; the
+// exit protocol costs a few microseconds per CTA, so short launches and the
+// other passes keep the static order).  The last CTA to leave resets both words,
+// so the next launch on the stream (or the next replay of a graph) starts
+// from zero without a host-side reset.
+// With no counter (tctr null) the k-th ticket of a CTA is the static
+// blockIdx.x + k gridDim.x.
+__device__ __forceinline__ int tile_ticket(int* tctr, int k) {
+    return tctr ? atomicAdd(tctr, 1) : (int)blockIdx.x + k * (int)gridDim.x;
+}
+__device__ __forceinline__ void tile_tickets_done(int* tctr, int tid) {
+    if (tctr && tid == 0) {
+        __threadfence();
+        if (atomicAdd(tctr + 1, 1) == (int)gridDim.x - 1) {
+            tctr[0] = 0;
+            tctr[1] = 0;
+            __threadfence();
+        }
     }
 }
 
@@ -370,7 +394,7 @@ __device__ __forceinline__ void col_last_store(const cpx<T>* tile, int tid, cons
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(col_threads<T, N, MODE>(), col_ctas<T, N, MODE>())
 col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
-         int ntx, int tiles_per, int ntiles) {
+         int ntx, int tiles_per, int ntiles, int* __restrict__ tctr) {
     constexpr int NT = col_threads<T, N, MODE>();
     constexpr int NBUF = col_nbuf<T, N, MODE>();
     constexpr int NB = col_nb(MODE);
@@ -395,7 +419,16 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     for (int i = tid; i < N; i += NT) tw[i] = tw_g[i];
 
     // tile t: member t / tiles_per, then (a, kx-tile) with the kx-tile fastest
-    int t = blockIdx.x;
+    // tiles: this one (t) and, with two buffers, the next one (tnext)
+    __shared__ int s_tk[2];
+    int nk = 0;  // tickets drawn (thread 0)
+    if (tid == 0) {
+        s_tk[0] = tile_ticket(tctr, nk++);
+        s_tk[1] = NBUF == 2 ? tile_ticket(tctr, nk++) : 0;
+    }
+    __syncthreads();
+    int t = s_tk[0];
+    int tnext = s_tk[1];
     if (t < ntiles) {
         const int m = t / tiles_per, tl = t - m * tiles_per;
         const int kx0 = (tl % ntx) * TKX;
@@ -404,7 +437,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     }
     cp_async_commit();
     __shared__ Member<T> mb;  // this tile's member, read once per tile
-    for (int it = 0; t < ntiles; ++it, t += gridDim.x) {
+    for (int it = 0; t < ntiles; ++it) {
         cpx<T>* tile = bufs + (NBUF == 2 ? (it & 1) * TILE : 0);
         const int m = t / tiles_per, tl = t - m * tiles_per;
         {
@@ -436,7 +469,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         }
         if constexpr (NBUF == 2) {
             // the next tile streams into the other buffer while this one is transformed
-            const int tn = t + gridDim.x;
+            const int tn = tnext;
             if (tn < ntiles) {
                 const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
                 const int kx0n = (tln % ntx) * TKX;
@@ -450,6 +483,9 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         else if constexpr (NBUF == 2) cp_async_wait<1>();
         else cp_async_wait<0>();
         __syncthreads();
+        // ticket for the tile after the prefetched one (two buffers) or for
+        // the next one (one buffer); read after the barrier ending this tile
+        if (tid == 0) s_tk[0] = tile_ticket(tctr, nk++);
         const int a = tl / ntx;
         const int kx0 = (tl % ntx) * TKX;
         const int ncol = min(TKX, NXV - kx0);
@@ -519,7 +555,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         }
         __syncthreads();  // this buffer is refilled by the next load
         if constexpr (NBUF == 1) {
-            const int tn = t + gridDim.x;
+            const int tn = s_tk[0];
             if (tn < ntiles) {
                 const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
                 const int kx0n = (tln % ntx) * TKX;
@@ -527,9 +563,15 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                                            tln / ntx, kx0n, min(TKX, NXV - kx0n), nxp3, tid);
             }
             cp_async_commit();
+            t = tn;
+        } else {
+            const int t2 = s_tk[0];
+            t = tnext;
+            tnext = t2;
         }
     }
     cp_async_wait<0>();
+    tile_tickets_done(tctr, tid);
 }
 
 // ---------------------------------------------------------------------------
