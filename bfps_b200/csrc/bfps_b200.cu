@@ -1430,8 +1430,8 @@ struct bfg_ens {
     // re-sorting); the others use their own loop
     std::vector<int> batched;   // entry indices
     void* dsets = nullptr;      // TracerSet[batched.size()]
-    void* dstart = nullptr;     // int64[batched.size() + 1]
-    int64_t nbatched = 0;
+    void* dstart = nullptr;     // int64[batched.size() + 1]: first block of each set
+    int64_t nbatched = 0;       // blocks of the batched tracer launch
     bool dirty = true;
     bool use_graphs = true;
     int* tctr = nullptr;  // tile counters of the launches on this stream
@@ -1445,7 +1445,7 @@ static int ens_fail(bfg_ens* e, int code, const char* msg) {
 
 template <typename T, int NB, int MM>
 static int ens_tracers_launch(bfg_ens* e) {
-    const unsigned blocks = (unsigned)((e->nbatched + TRACER_THREADS - 1) / TRACER_THREADS);
+    const unsigned blocks = (unsigned)e->nbatched;  // blocks over all sets
     if (blocks == 0) return 0;
     tracer_batch_kernel<T, NB, MM><<<blocks, TRACER_THREADS, 0, e->stream>>>(
         (const TracerSet*)e->dsets, (const int64_t*)e->dstart, (int)e->batched.size());
@@ -1612,7 +1612,7 @@ static int ens_prepare(bfg_ens* e) {
         ts.pos = p->pos;
         ts.hist = p->hist;
         sets.push_back(ts);
-        start.push_back(start.back() + p->n);
+        start.push_back(start.back() + (p->n + TRACER_THREADS - 1) / TRACER_THREADS);
         e->batched.push_back(i);
     }
     if (!sets.empty()) {

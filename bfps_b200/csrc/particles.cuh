@@ -340,20 +340,36 @@ __global__ void tracer_sets_advance(TracerSet* __restrict__ sets, int nsets) {
     s.pp.accum = 0;
 }
 
+// Each set owns whole blocks: block b belongs to the set k with
+// bstart[k] <= b < bstart[k+1]; the set is found once per block and its
+// descriptor copied to shared memory.
 template <typename T, int NB, int MM>
 __global__ void __launch_bounds__(TRACER_THREADS)
-tracer_batch_kernel(const TracerSet* __restrict__ sets, const int64_t* __restrict__ start,
+tracer_batch_kernel(const TracerSet* __restrict__ sets, const int64_t* __restrict__ bstart,
                     int nsets) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= start[nsets]) return;
-    int lo = 0, hi = nsets - 1;
-    while (lo < hi) {  // last k with start[k] <= i
-        const int mid = (lo + hi + 1) / 2;
-        if (start[mid] <= i) lo = mid;
-        else hi = mid - 1;
+    __shared__ TracerSet s;
+    __shared__ int s_k;
+    if (threadIdx.x == 0) {
+        const int64_t b = blockIdx.x;
+        int lo = 0, hi = nsets - 1;
+        while (lo < hi) {  // last k with bstart[k] <= b
+            const int mid = (lo + hi + 1) / 2;
+            if (bstart[mid] <= b) lo = mid;
+            else hi = mid - 1;
+        }
+        s_k = lo;
     }
-    const TracerSet& s = sets[lo];
-    tracer_one<T, NB, MM>(s.pp, (const T*)s.ru, s.pos, s.hist, nullptr, i - start[lo]);
+    __syncthreads();
+    {
+        static_assert(sizeof(TracerSet) % 4 == 0, "descriptor copy");
+        const int* src = reinterpret_cast<const int*>(&sets[s_k]);
+        int* dst = reinterpret_cast<int*>(&s);
+        for (int w = threadIdx.x; w < (int)(sizeof(TracerSet) / 4); w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int64_t i = ((int64_t)blockIdx.x - bstart[s_k]) * blockDim.x + threadIdx.x;
+    if (i >= s.pp.n) return;
+    tracer_one<T, NB, MM>(s.pp, (const T*)s.ru, s.pos, s.hist, nullptr, i);
 }
 
 // ---------------------------------------------------------------------------
