@@ -1184,7 +1184,11 @@ int bfg_particles_download(bfg_pctx* p, double* pos, double* rhs, int64_t* idx) 
     if (rhs) {
         for (int j = 0; j < p->nsteps; ++j) {
             if (j == 0 && p->rhs0_zero) {
-                std::fill(rhs, rhs + n3, 0.0);
+                // logically zero slot: zeros through the link (faster than a
+                // host fill of the caller's buffer)
+                CU(cudaMemsetAsync(p->pos2, 0, n3 * 8, c->stream));
+                CU(cudaMemcpyAsync(rhs, p->pos2, n3 * 8, cudaMemcpyDeviceToHost, c->stream));
+                CU(cudaStreamSynchronize(c->stream));
                 continue;
             }
             const int slot = (p->head + j) % p->nsteps;
@@ -1213,10 +1217,10 @@ int bfg_particles_upload(bfg_pctx* p, const double* pos, const double* rhs, int 
     // back to creation order, then cell order
     CU(cudaMemcpyAsync(p->pos, pos, n3 * 8, cudaMemcpyHostToDevice, c->stream));
     if (rhs) {
+        // rhs[0] as given: the next loop accumulates into it (rhs[0] += u(x),
+        // completeLoop's own form; exact when the slot holds zeros)
         CU(cudaMemcpyAsync(p->hist, rhs, n3 * 8 * p->nsteps, cudaMemcpyHostToDevice, c->stream));
-        bool z = true;
-        for (size_t i = 0; i < n3 && z; ++i) z = rhs[i] == 0.0;
-        p->rhs0_zero = z;
+        p->rhs0_zero = false;
     } else {
         CU(cudaMemsetAsync(p->hist, 0, n3 * 8 * p->nsteps, c->stream));
         p->rhs0_zero = true;
