@@ -45,6 +45,8 @@ SIGNATURES = {
     "bfg_read_checkpoint_fixup": (_i, [_vp]),
     "bfg_step": (_i, [_vp, _d, _i]),
     "bfg_compute_velocity": (_i, [_vp]),
+    "bfg_compute_pressure": (_i, [_vp, _vp]),
+    "bfg_lagrangian_acceleration": (_i, [_vp, _vp]),
     "bfg_velocity_rspace": (_i, [_vp]),
     "bfg_ift": (_i, [_vp, _vp, _vp]),
     "bfg_dft": (_i, [_vp, _vp, _vp]),
@@ -56,6 +58,7 @@ SIGNATURES = {
     "bfg_particles_complete_loop": (_i, [_vp, _d]),
     "bfg_nsveparticles_step": (_i, [_vp, _vp, _d, _i]),
     "bfg_particles_sample_velocity": (_i, [_vp, _pd]),
+    "bfg_particles_sample_acceleration": (_i, [_vp, _pd]),
     "bfg_particles_download": (_i, [_vp, _pd, _pd, _pi64]),
     "bfg_particles_upload": (_i, [_vp, _pd, _pd, _i]),
     "bfg_profile": (_i, [_vp, _i]),

@@ -17,6 +17,7 @@
 #include "bfps_b200.h"
 #include "particles.cuh"
 #include "passes.cuh"
+#include "pressure.cuh"
 #include "stats.cuh"
 
 using namespace bfg;
@@ -355,6 +356,63 @@ struct Engine {
         return col<CM_FZ_PLAIN>(c, self(c), 1, roles(B_WA, B_NONE, B_WB, B_NONE));
     }
 
+    // real-space products of the velocity in ru into v2 (as reals [z][y][x][3])
+    static int products(bfg_ctx* c, int off) {
+        const size_t npts = (size_t)N * N * N;
+        Prof pr(c, K_KSPACE);
+        products_kernel<T><<<(unsigned)((npts + 255) / 256), 256, 0, c->stream>>>(
+            (const T*)c->ru, (T*)c->v2, npts, off);
+        return after_launch(c, "products");
+    }
+    // unnormalised R2C of v2 (reals) into wb (state layout); uses wa
+    static int dft_v2(bfg_ctx* c) {
+        int rc;
+        if ((rc = row<RM_R2C, false>(c, self(c), 1, roles(B_NONE, B_NONE, B_WA, B_NONE, B_NONE,
+                                                          B_NONE, B_NONE, B_NONE, B_V2))))
+            return rc;
+        if ((rc = col<CM_Y_FWD1>(c, self(c), 1, roles(B_WA, B_NONE, B_WA, B_NONE)))) return rc;
+        return col<CM_FZ_PLAIN>(c, self(c), 1, roles(B_WA, B_NONE, B_WB, B_NONE));
+    }
+    // vorticity_equation::compute_pressure (vorticity_equation.cpp:441-514)
+    // of the current state's velocity: p^ into component 0 of v1; ru holds
+    // u(x) afterwards
+    static int pressure(bfg_ctx* c) {
+        int rc;
+        if ((rc = velocity_rspace(c))) return rc;
+        const size_t nm = (size_t)N * N * c->nxv;
+        for (int off = 0; off < 2; ++off) {
+            if ((rc = products(c, off))) return rc;
+            if ((rc = dft_v2(c))) return rc;
+            Prof pr(c, K_KSPACE);
+            pressure_kernel<T, N><<<(unsigned)((nm + 255) / 256), 256, 0, c->stream>>>(
+                kparams(c, 0.0), (const T*)c->filt, (const C*)c->wb, (C*)c->v1, off);
+            if ((rc = after_launch(c, "pressure"))) return rc;
+        }
+        return 0;
+    }
+    // compute_Lagrangian_acceleration (vorticity_equation.cpp:516-578): a^
+    // into wb (state layout); u^ of the current state (symmetrised, as
+    // compute_velocity does) in wa
+    static int acceleration(bfg_ctx* c) {
+        int rc;
+        if ((rc = pressure(c))) return rc;
+        if ((rc = velocity_state(c))) return rc;
+        const size_t nm = (size_t)N * N * c->nxv;
+        Prof pr(c, K_KSPACE);
+        acceleration_kernel<T, N><<<(unsigned)((nm + 255) / 256), 256, 0, c->stream>>>(
+            kparams(c, 0.0), c->nu, (const C*)c->wa, (const C*)c->v1, (C*)c->wb);
+        return after_launch(c, "acceleration");
+    }
+    // the acceleration in real space into v2 (reals [z][y][x][3]); uses wa
+    static int acceleration_rspace(bfg_ctx* c) {
+        int rc;
+        if ((rc = acceleration(c))) return rc;
+        if ((rc = col<CM_IZ_PLAIN>(c, self(c), 1, roles(B_WB, B_NONE, B_WA, B_NONE)))) return rc;
+        if ((rc = col<CM_Y_INV1>(c, self(c), 1, roles(B_WA, B_NONE, B_WA, B_NONE)))) return rc;
+        return row<RM_C2R, false>(c, self(c), 1, roles(B_WA, B_NONE, B_NONE, B_NONE, B_NONE, B_NONE,
+                                                       B_NONE, B_V2));
+    }
+
     static int stats(bfg_ctx* c, int cfield, double max_est, int nbins, double* spec, double* mom,
                      int64_t* hist);
 };
@@ -399,6 +457,18 @@ struct OpVelocity {
 template <typename T, int N>
 struct OpVelocityR {
     static int run(bfg_ctx* c) { return Engine<T, N>::velocity_rspace(c); }
+};
+template <typename T, int N>
+struct OpPressure {
+    static int run(bfg_ctx* c) { return Engine<T, N>::pressure(c); }
+};
+template <typename T, int N>
+struct OpAccel {
+    static int run(bfg_ctx* c) { return Engine<T, N>::acceleration(c); }
+};
+template <typename T, int N>
+struct OpAccelR {
+    static int run(bfg_ctx* c) { return Engine<T, N>::acceleration_rspace(c); }
 };
 template <typename T, int N>
 struct OpFixup {
@@ -577,20 +647,21 @@ static int ensure_ru(bfg_ctx* c) {
 // ----------------------------------------------------------- tracers --
 template <typename T, int NB, int MM>
 static int launch_tracers(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out,
-                          cudaStream_t st) {
+                          cudaStream_t st, const void* field) {
     const unsigned blocks = (unsigned)((p->n + TRACER_THREADS - 1) / TRACER_THREADS);
     if (blocks == 0) return 0;
     Prof pr(c, K_TRACER, st);
     tracer_kernel<T, NB, MM><<<blocks, TRACER_THREADS, 0, st>>>(
-        pp, (const T*)c->ru, p->pos, p->hist, out);
+        pp, (const T*)(field ? field : c->ru), p->pos, p->hist, out);
     return after_launch(c, "tracer_kernel");
 }
 
 template <typename T>
 static int tracers_dispatch(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out,
-                            cudaStream_t st) {
+                            cudaStream_t st, const void* field = nullptr) {
 #define BFG_TR(NBv, MMv) \
-    if (p->neighbours == NBv && p->smoothness == MMv) return launch_tracers<T, NBv, MMv>(c, pp, p, out, st);
+    if (p->neighbours == NBv && p->smoothness == MMv) \
+        return launch_tracers<T, NBv, MMv>(c, pp, p, out, st, field);
     BFG_TR(1, 0) BFG_TR(1, 1) BFG_TR(1, 2)
     BFG_TR(2, 0) BFG_TR(2, 1) BFG_TR(2, 2)
     BFG_TR(3, 0) BFG_TR(3, 1) BFG_TR(3, 2)
@@ -934,6 +1005,52 @@ int bfg_velocity_rspace(bfg_ctx* c) {
     return 0;
 }
 
+// a state-layout device buffer (csrc components per point) to the
+// reference host layout with cout components, through the staging buffer
+static int download_state(bfg_ctx* c, const void* src, int csrc, int cout, void* host,
+                          void* staging) {
+    const size_t rows = (size_t)c->n * c->n;
+    const size_t n = rows * c->nxv * cout;
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (c->real_bytes == 4)
+        gather_rows_kernel<float><<<blocks, 256, 0, c->stream>>>(
+            (const cpx<float>*)src, c->nxp, c->nxv, csrc, cout, (cpx<float>*)staging, rows);
+    else
+        gather_rows_kernel<double><<<blocks, 256, 0, c->stream>>>(
+            (const cpx<double>*)src, c->nxp, c->nxv, csrc, cout, (cpx<double>*)staging, rows);
+    int rc = after_launch(c, "gather_rows");
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(host, staging, n * 2 * c->real_bytes, cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_compute_pressure(bfg_ctx* c, void* host) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
+    if ((rc = dispatch<OpPressure>(c))) return rc;
+    if (host) return download_state(c, c->v1, 3, 1, host, c->v2);
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_lagrangian_acceleration(bfg_ctx* c, void* host) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
+    if ((rc = dispatch<OpAccel>(c))) return rc;
+    if (host) return download_state(c, c->wb, 3, 3, host, c->v2);
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
 int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
     if (!c || !din || !dout) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
@@ -1169,6 +1286,22 @@ int bfg_particles_sample_velocity(bfg_pctx* p, double* out) {
     PParams pp = pparams(p, 0.0, 0);
     int rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, p->sample, c->stream)
                                 : tracers_dispatch<double>(c, pp, p, p->sample, c->stream);
+    if (rc) return rc;
+    return fetch_index_order(p, p->sample, 3, out);
+}
+
+int bfg_particles_sample_acceleration(bfg_pctx* p, double* out) {
+    if (!p || !out) return BFG_EINVAL;
+    bfg_ctx* c = p->ctx;
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
+    if ((rc = dispatch<OpAccelR>(c))) return rc;
+    PParams pp = pparams(p, 0.0, 0);
+    rc = c->real_bytes == 4 ? tracers_dispatch<float>(c, pp, p, p->sample, c->stream, c->v2)
+                            : tracers_dispatch<double>(c, pp, p, p->sample, c->stream, c->v2);
     if (rc) return rc;
     return fetch_index_order(p, p->sample, 3, out);
 }

@@ -159,6 +159,20 @@ class vorticity_equation:
     def velocity_rspace(self):
         check(lib().bfg_velocity_rspace(self._h), self._h)
 
+    def compute_pressure(self):
+        """vorticity_equation::compute_pressure (vorticity_equation.cpp:441-514)
+        of the current state's velocity, (ny, nz, nx/2+1) complex."""
+        out = np.empty(self.cshape[:3], self.cdtype)
+        check(lib().bfg_compute_pressure(self._h, out.ctypes.data), self._h)
+        return out
+
+    def compute_Lagrangian_acceleration(self):
+        """vorticity_equation::compute_Lagrangian_acceleration
+        (vorticity_equation.cpp:516-578) of the current state, Fourier space."""
+        out = np.empty(self.cshape, self.cdtype)
+        check(lib().bfg_lagrangian_acceleration(self._h, out.ctypes.data), self._h)
+        return out
+
     def last_step_ms(self):
         ms = ctypes.c_double()
         check(lib().bfg_last_step_ms(self._h, ctypes.byref(ms)), self._h)
@@ -222,6 +236,13 @@ class particles_system:
     def sample_velocity(self):
         out = np.empty((self.n, 3))
         check(lib().bfg_particles_sample_velocity(self._h, ptr(out)), self.fs.handle)
+        return out
+
+    def sample_acceleration(self):
+        """Lagrangian acceleration of the current state at the tracers
+        (NSVEparticles::do_stats, NSVEparticles.cpp:84-91), (n, 3)."""
+        out = np.empty((self.n, 3))
+        check(lib().bfg_particles_sample_acceleration(self._h, ptr(out)), self.fs.handle)
         return out
 
     def state(self):

@@ -103,6 +103,18 @@ int bfg_compute_velocity(bfg_ctx* ctx);
  * (NSVEparticles.cpp:35-36): fills BFG_FIELD_RVELOCITY. */
 int bfg_velocity_rspace(bfg_ctx* ctx);
 
+/* vorticity_equation::compute_pressure (vorticity_equation.cpp:441-514) of
+ * the velocity of the current state (compute_velocity + ift first, as
+ * compute_Lagrangian_acceleration does at :528-531).  If host is not NULL
+ * the pressure is written there in the reference complex layout
+ * (ny, nz, nx/2+1) of one component.  Leaves BFG_FIELD_RVELOCITY set. */
+int bfg_compute_pressure(bfg_ctx* ctx, void* host);
+
+/* vorticity_equation::compute_Lagrangian_acceleration
+ * (vorticity_equation.cpp:516-578) of the current state, in Fourier space;
+ * written to host (reference layout (ny, nz, nx/2+1, 3)) if not NULL. */
+int bfg_lagrangian_acceleration(bfg_ctx* ctx, void* host);
+
 /* field::ift / field::dft (field.cpp:144-162) on a 3-vector field, using
  * caller device buffers in the reference layouts (complex: (n, n, n/2+1, 3),
  * real: (n, n, n+2, 3)); unnormalised like FFTW.  in may equal out. */
@@ -149,6 +161,12 @@ int bfg_nsveparticles_step(bfg_ctx* ctx, bfg_pctx* p, double dt, int nsteps);
  * (particles_system::sample_compute, particles_system.hpp:134-170) into
  * out (n, 3) in global index order. */
 int bfg_particles_sample_velocity(bfg_pctx* p, double* out);
+
+/* The acceleration half of NSVEparticles::do_stats (NSVEparticles.cpp:
+ * 84-91): compute_Lagrangian_acceleration of the current state, ift, and
+ * sample it at the tracer positions into out (n, 3) in global index order
+ * (the context's real velocity field is left untouched). */
+int bfg_particles_sample_acceleration(bfg_pctx* p, double* out);
 
 /* Replace positions (n, 3) and the rhs history (nsteps, n, 3, NULL for
  * zeros) of existing tracers, in the order given at creation, and set

@@ -19,7 +19,8 @@ Everything follows the reference line by line; citations are
 * dealias / low_pass / force_divfree / cospectrum (kspace.cpp:235-253,
   461-598).
 * compute_velocity, add_forcing, omega_nonlin, IF-RK3 step
-  (vorticity_equation.cpp:206-439).
+  (vorticity_equation.cpp:206-439); compute_pressure and
+  compute_Lagrangian_acceleration (vorticity_equation.cpp:441-578).
 * symmetrize (field.cpp:903-978), impose_zero_mode (field.hpp:226-233).
 * real-space moments and histograms (field.cpp:661-889) and
   compute_stats (field.cpp:984-1040).
@@ -332,6 +333,62 @@ class VorticityEquation:
         kk.force_divfree(self.cvorticity)
         symmetrize(self.cvorticity)
         self.iteration += 1
+
+    def compute_pressure(self, ur):
+        """vorticity_equation.cpp:441-514: pressure (one complex component,
+        ``(ny, nz, nx/2+1)``) from the real-space velocity ``ur``
+        ((nz, ny, nx, 3), unnormalised inverse transform of u^).  The
+        dealiased transforms of u_c u_c (diagonal) and u_c u_(c+1)
+        (off-diagonal) are contracted with k_i k_j; p = 0 outside
+        0 < k2 <= kM2; finally p /= npoints k2."""
+        kk = self.kk
+        u = ur.astype(np.float64)
+        k2 = kk.K2
+        m = (k2 <= kk.kM2) & (k2 > 0)
+        kx, ky, kz = kk.KX, kk.KY, kk.KZ
+        rd = self.rdtype
+        # diagonal terms 11 22 33 (:451-480)
+        d = np.empty_like(u)
+        for cc in range(3):
+            d[..., cc] = u[..., cc] * u[..., cc]
+        G = self._store(self.dft(d.astype(rd))).astype(np.complex128)
+        kk.dealias(G)
+        G = self._store(G).astype(np.complex128)
+        p = -(kx * kx * G[..., 0] + ky * ky * G[..., 1] + kz * kz * G[..., 2])
+        p = np.where(m, p, 0)
+        p = p.astype(self.cdtype).astype(np.complex128)
+        # off-diagonal terms 12 23 31 (:481-513)
+        for cc in range(3):
+            d[..., cc] = u[..., cc] * u[..., (cc + 1) % 3]
+        G = self._store(self.dft(d.astype(rd))).astype(np.complex128)
+        kk.dealias(G)
+        G = self._store(G).astype(np.complex128)
+        q = p - 2 * (kx * ky * G[..., 0] + ky * kz * G[..., 1] + kz * kx * G[..., 2])
+        q = q.astype(self.cdtype).astype(np.complex128)
+        safe = np.where(m, k2, 1.0)
+        q = q / (self.npoints * safe)
+        return np.where(m, q, p).astype(self.cdtype)
+
+    def compute_lagrangian_acceleration(self):
+        """vorticity_equation.cpp:516-578: acceleration in Fourier space,
+        a = -nu k2 u^ (+ famplitude u^ on the linear forcing band) - i k p^
+        for k2 <= kM2, else 0; u^ from the current vorticity."""
+        kk = self.kk
+        u = self.compute_velocity(self.cvorticity)
+        p = self.compute_pressure(self.ift(u)).astype(np.complex128)
+        u = self.compute_velocity(self.cvorticity).astype(np.complex128)
+        k2 = kk.K2
+        m = k2 <= kk.kM2
+        a = -self.nu * k2[..., None] * u
+        a = a.astype(self.cdtype).astype(np.complex128)
+        if self.forcing_type == "linear":
+            band = m & (self.fk0 <= self._knorm) & (self.fk1 >= self._knorm)
+            a[band] += self.famplitude * u[band]
+            a = a.astype(self.cdtype).astype(np.complex128)
+        for c, kc in enumerate((kk.KX, kk.KY, kk.KZ)):
+            a[..., c] = (a[..., c].real + kc * p.imag) + 1j * (a[..., c].imag - kc * p.real)
+        a[~m] = 0
+        return a.astype(self.cdtype)
 
     def read_checkpoint_semantics(self, c):
         """What io_checkpoint(read) does to a field read from a file:
