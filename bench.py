@@ -210,6 +210,38 @@ def build_solver(cfg, w0, pos, device):
     return ve, ps
 
 
+def acceleration_report(ve, ps, cfg, reps=3):
+    """NSVEparticles::do_stats acceleration sampling (pressure, Lagrangian
+    acceleration, inverse transform, tracer gather) on the current state:
+    device time per call from per-launch CUDA events, and achieved bandwidth
+    against its algorithmic bytes, 109 U + 48 n (19 launches: velocity to
+    real space 18U, two products 12U, two forward transforms 36U, two
+    pressure contractions 9U, velocity 6U, acceleration 7U, inverse
+    transform 18U, gather 3U + 48 n)."""
+    from bfps_b200 import _lib
+    L = _lib.lib()
+    out = np.empty((ps.n, 3))
+    L.bfg_particles_sample_acceleration(ps.handle, _lib.ptr(out))
+    L.bfg_profile(ve.handle, 1)
+    for _ in range(reps):
+        L.bfg_particles_sample_acceleration(ps.handle, _lib.ptr(out))
+    tot, n = 0.0, 0
+    for k in range(len(KIND_NAMES)):
+        t, c = _lib.ctypes.c_double(), _lib.ctypes.c_int64()
+        L.bfg_profile_read(ve.handle, k, _lib.ctypes.byref(t), _lib.ctypes.byref(c))
+        tot += t.value
+        n += c.value
+    L.bfg_profile(ve.handle, 0)
+    ms = tot / reps
+    P = 4 if cfg["precision"] == "single" else 8
+    U = cfg["n"] ** 2 * (cfg["n"] + 2) * P
+    nbytes = 109 * U + 48 * ps.n
+    peak, _ = peaks()
+    return {"device_ms": round(ms, 3), "launches_per_call": n // reps,
+            "algorithmic_bytes": int(nbytes), "achieved_gbs": round(nbytes / (ms / 1e3) / 1e9, 1),
+            "frac_of_peak": round(nbytes / (ms / 1e3) / 1e9 / peak, 4)}
+
+
 def precision_report(cfg, w0, pos, device, nsteps):
     """Precision form against FP64: the same initial field (the FP32-rounded
     one) and tracers stepped nsteps times in FP32 and in FP64; relative error
@@ -370,6 +402,8 @@ def run_ours(args, cfg):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if ps.n > 0 and world == 1:
+        out["acceleration_sampling"] = acceleration_report(ve, ps, cfg)
     ps.close()
     ve.close()
     if cfg.get("accuracy_steps") and cfg["precision"] == "single" and not args.no_precision:
