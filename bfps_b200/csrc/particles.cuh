@@ -311,7 +311,7 @@ __device__ __forceinline__ void tracer_one(const PParams& pp, const T* __restric
 }
 
 template <typename T, int NB, int MM>
-__global__ void __launch_bounds__(TRACER_THREADS)
+__global__ void __launch_bounds__(TRACER_THREADS, 6)
 tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ pos,
               double* __restrict__ hist, double* __restrict__ sample_out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
