@@ -158,35 +158,19 @@ class ClockSampler:
 
 
 def dist_setup(ngpus):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-    return world, rank, local, pg
+    """Replica ranks (bfps_b200.replicas): NCCL over the GPUs of one node."""
+    from bfps_b200 import replicas
+    return replicas.setup("nccl")
 
 
 def barrier(pg):
-    if pg is not None:
-        import torch
-        pg.barrier()
-        torch.cuda.synchronize()
+    from bfps_b200 import replicas
+    replicas.barrier(pg)
 
 
 def allmax(pg, v):
-    if pg is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    from bfps_b200 import replicas
+    return replicas.allmax(pg, v)
 
 
 def make_inputs(cfg, seed):
