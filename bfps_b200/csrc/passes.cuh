@@ -215,16 +215,45 @@ __device__ __forceinline__ size_t col_out_row(int a, int lo) {
 //      per axis (their product over the axes is the factor of k^2).
 // FZ epilogue for one mode (l = kz, ix): dealias, i k x, forcing,
 // force_divfree, RK update of stage MODE (vorticity_equation.cpp:290-437)
+// What an epilogue mode needs from its kx column and the tile's ky: computed
+// once per column (a thread keeps one column over its modes).
+template <typename T>
+struct FzCol {
+    double kx, ky, kxy2;  // kx, ky, kx^2 + ky^2
+    T kxT, kyT;
+    T fxy0, fxy1;         // kx and ky parts of the integrating factors
+    double lo, hi;        // forcing band on k2 (see fz_point)
+};
+template <typename T, int N, int MODE>
+__device__ __forceinline__ FzCol<T> fz_col(const KParams& kp, const T* __restrict__ fac, int a,
+                                           int ix, double ky) {
+    FzCol<T> fc;
+    fc.kx = (double)ix * kp.dkx;
+    fc.ky = ky;
+    fc.kxy2 = fc.kx * fc.kx + ky * ky;
+    fc.kxT = (T)fc.kx;
+    fc.kyT = (T)ky;
+    const int nxv = kp.nxv, nfac = nxv + 2 * N;
+    const int s0 = MODE == CM_FZ_RK1 ? 0 : 1;
+    fc.fxy0 = fac[s0 * nfac + ix] * fac[s0 * nfac + nxv + a];
+    fc.fxy1 = MODE == CM_FZ_RK2 ? fac[2 * nfac + ix] * fac[2 * nfac + nxv + a] : (T)0;
+    // the band test on |k| = sqrt(k2), taken only where k2 is near the band
+    // (the margin keeps every mode the exact test accepts)
+    fc.lo = kp.fk0 > 0.0 ? kp.fk0 * kp.fk0 * (1.0 - 1e-12) : -1.0;
+    fc.hi = kp.fk1 * kp.fk1 * (1.0 + 1e-12);
+    return fc;
+}
+
 template <typename T, int N, int MODE>
 __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, int PR, int a, int l,
-                                         int ix, int col, double ky, const cpx<T>* v0,
+                                         int ix, int col, const FzCol<T>& fc, const cpx<T>* v0,
                                          const cpx<T>* vp, size_t pt, const T* __restrict__ filt,
                                          const T* __restrict__ fac, const cpx<T>* __restrict__ fsrc,
                                          cpx<T>* out0) {
     const int nxv = kp.nxv;
     const double kz = kwrap<N>(l, kp.dkz);
-    const double kx = (double)ix * kp.dkx;
-    const double k2 = (kx * kx + ky * ky) + kz * kz;
+    const double kx = fc.kx, ky = fc.ky;
+    const double k2 = fc.kxy2 + kz * kz;
     const int p = dif_position<N>(l);
     cpx<T> nl[3];
 #pragma unroll
@@ -242,14 +271,11 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     }
     // i k x (vorticity_equation.cpp:323-350)
     cpx<T> tt[3];
-    curl<T>((T)kx, (T)ky, (T)kz, nl, tt);
+    const T kzT = (T)kz;
+    curl<T>(fc.kxT, fc.kyT, kzT, nl, tt);
     // forcing (vorticity_equation.cpp:241-288), factor 1
     if (kp.forcing == 1) {
-        // the band test on |k| = sqrt(k2), taken only where k2 is near the
-        // band (the margin keeps every mode the exact test accepts)
-        const double lo = kp.fk0 > 0.0 ? kp.fk0 * kp.fk0 * (1.0 - 1e-12) : -1.0;
-        const double hi = kp.fk1 * kp.fk1 * (1.0 + 1e-12);
-        if (k2 >= lo && k2 <= hi && kp.fk0 <= sqrt(k2) && kp.fk1 >= sqrt(k2)) {
+        if (k2 >= fc.lo && k2 <= fc.hi && kp.fk0 <= sqrt(k2) && kp.fk1 >= sqrt(k2)) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const cpx<T> fv = fsrc[pt * 3 + c];
@@ -265,7 +291,7 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     }
     // force_divfree on the nonlinear term; zero mode cleared
     const bool kzero = (a == 0 && l == 0 && ix == 0);
-    if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)__drcp_rn(k2), tt);
+    if (k2 > 0.0) divfree<T>(fc.kxT, fc.kyT, kzT, (T)__drcp_rn(k2), tt);
     if (kzero) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) tt[c] = zero_c<T>();
@@ -276,14 +302,14 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     cpx<T> o[3];
     const int nfac = nxv + 2 * N;
     if (MODE == CM_FZ_RK1) {
-        const T f0 = fac[ix] * fac[nxv + a] * fac[nxv + N + l];
+        const T f0 = fc.fxy0 * fac[nxv + N + l];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
             o[c] = inside ? mk<T>((v0[c].x + dt * tt[c].x) * f0, (v0[c].y + dt * tt[c].y) * f0)
                           : zero_c<T>();
     } else if (MODE == CM_FZ_RK2) {
-        const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
-        const T f1 = fac[2 * nfac + ix] * fac[2 * nfac + nxv + a] * fac[2 * nfac + nxv + N + l];
+        const T f0 = fc.fxy0 * fac[nfac + nxv + N + l];
+        const T f1 = fc.fxy1 * fac[2 * nfac + nxv + N + l];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
             o[c] = inside ? mk<T>((3 * v0[c].x * f0 + (vp[c].x + dt * tt[c].x) * f1) * (T)0.25,
@@ -291,14 +317,14 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
                           : zero_c<T>();
     } else {
         const T third = (T)(1.0 / 3.0);  // the division by 3 as a product (within one rounding)
-        const T f0 = fac[nfac + ix] * fac[nfac + nxv + a] * fac[nfac + nxv + N + l];
+        const T f0 = fc.fxy0 * fac[nfac + nxv + N + l];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
             o[c] = inside ? mk<T>((v0[c].x * f0 + 2 * (vp[c].x + dt * tt[c].x)) * f0 * third,
                                   (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 * third)
                           : v0[c];
         // final force_divfree of the state (vorticity_equation.cpp:436)
-        if (k2 > 0.0) divfree<T>((T)kx, (T)ky, (T)kz, (T)__drcp_rn(k2), o);
+        if (k2 > 0.0) divfree<T>(fc.kxT, fc.kyT, kzT, (T)__drcp_rn(k2), o);
         if (kzero) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
@@ -534,15 +560,27 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             __syncthreads();
             // ---- epilogue: one thread per mode (kz = l, kx = kx0 + col)
             const double ky = kwrap<N>(a, kp.dky);
-            for (int e = tid; e < N * TKX; e += NT) {
-                const int col = e % TKX;
-                const int l = e / TKX;
-                if (col >= ncol) continue;
+            auto mode = [&](int col, int l, const FzCol<T>& fc) {
                 const size_t pt = ((size_t)a * N + l) * (N / 2 + 4) + kx0 + col;  // S[ky=a][kz=l][kx]
                 const cpx<T>* v0 = &rkt[l * W + col * 3];
                 const cpx<T>* vp = &rkt[((NRK - 1) * N + l) * W + col * 3];
-                fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, ky, v0, vp, pt, mb.filt,
+                fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, fc, v0, vp, pt, mb.filt,
                                      mb.fac, mbuf(mb, rl.fsrc), mbuf(mb, rl.out0));
+            };
+            if constexpr (NT % TKX == 0) {
+                // a thread keeps one column: its constants once per tile
+                const int col = tid % TKX;
+                if (col < ncol) {
+                    const FzCol<T> fc = fz_col<T, N, MODE>(kp, mb.fac, a, kx0 + col, ky);
+                    for (int l = tid / TKX; l < N; l += NT / TKX) mode(col, l, fc);
+                }
+            } else {
+                for (int e = tid; e < N * TKX; e += NT) {
+                    const int col = e % TKX;
+                    const int l = e / TKX;
+                    if (col >= ncol) continue;
+                    mode(col, l, fz_col<T, N, MODE>(kp, mb.fac, a, kx0 + col, ky));
+                }
             }
         } else {
             if (ncol == TKX) {
