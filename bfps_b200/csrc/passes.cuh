@@ -521,19 +521,17 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         if constexpr (MODE == CM_IZ_VEL || MODE == CM_IZ_U) {
             constexpr int WSRC = (MODE == CM_IZ_VEL) ? W : 0;  // slot holding w^
             const double ky = kwrap<N>(a, kp.dky);
-            for (int e = tid; e < N * TKX; e += NT) {
-                const int col = e % TKX;
-                const int l = e / TKX;
-                if (col >= ncol) continue;
+            // one point: kx, kx^2 + ky^2 and the storage-precision kx, ky of its
+            // column given
+            auto point = [&](int col, int l, double kxy2, T kxT, T kyT) {
                 const double kz = kwrap<N>(l, kp.dkz);
-                const double kx = (double)(kx0 + col) * kp.dkx;
-                const double k2 = (kx * kx + ky * ky) + kz * kz;
+                const double k2 = kxy2 + kz * kz;
                 cpx<T>* w = &tile[l * PR + WSRC + col * 3];
                 cpx<T> u[3];
                 if (k2 <= kp.kM2 && k2 > 0.0) {
                     const T ik2 = (T)__drcp_rn(k2);
                     cpx<T> wv[3] = {w[0], w[1], w[2]};
-                    curl<T>((T)kx, (T)ky, (T)kz, wv, u);
+                    curl<T>(kxT, kyT, (T)kz, wv, u);
 #pragma unroll
                     for (int c = 0; c < 3; ++c) u[c] = scale(u[c], ik2);
                 } else {
@@ -542,6 +540,23 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 }
 #pragma unroll
                 for (int c = 0; c < 3; ++c) tile[l * PR + col * 3 + c] = u[c];
+            };
+            if constexpr (NT % TKX == 0) {
+                // a thread keeps one column
+                const int col = tid % TKX;
+                if (col < ncol) {
+                    const double kx = (double)(kx0 + col) * kp.dkx;
+                    const double kxy2 = kx * kx + ky * ky;
+                    for (int l = tid / TKX; l < N; l += NT / TKX) point(col, l, kxy2, (T)kx, (T)ky);
+                }
+            } else {
+                for (int e = tid; e < N * TKX; e += NT) {
+                    const int col = e % TKX;
+                    const int l = e / TKX;
+                    if (col >= ncol) continue;
+                    const double kx = (double)(kx0 + col) * kp.dkx;
+                    point(col, l, kx * kx + ky * ky, (T)kx, (T)ky);
+                }
             }
             __syncthreads();
         }
