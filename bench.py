@@ -452,8 +452,10 @@ def run_ensemble(args, cfg):
     clocks = ClockSampler(local)
     clocks.start()
     barrier(pg)
+    launches0 = ens.kernel_launches()
     ens.step(args.steps)
     ms = ens.last_ms()
+    launches = ens.kernel_launches() - launches0
     barrier(pg)
     clk = clocks.stop()
     ms = allmax(pg, ms)
@@ -516,7 +518,7 @@ def run_ensemble(args, cfg):
                        "how": "each instance stepped alone with the single-instance entry point"},
         "e2e": {"value": round(e2e_solves, 4), "unit": "solves/s", "h2d_bytes_per_step": int(nbytes),
                 "d2h_bytes_per_step": int(nbytes), "steps": e2e_steps},
-        "gpu_launches": None,
+        "gpu_launches": int(launches),
         "clocks": clk,
     }
     ens.close()
@@ -548,9 +550,11 @@ def run_serving(args, cfg):
     srv.run([w])
     srv.done.clear()
     barrier(pg)
+    launches0 = srv.ens.kernel_launches()
     t0 = time.perf_counter()
     done = srv.run(reqs)
     wall = time.perf_counter() - t0
+    launches = srv.ens.kernel_launches() - launches0
     srv.close()
     ttc = np.array([r.finished - r.arrival for r in done])
     span = max(r.finished for r in done) - min(r.arrival for r in done)
@@ -586,6 +590,7 @@ def run_serving(args, cfg):
         "e2e": {"value": round(solves_s * world, 4), "unit": "solves/s",
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                 "note": "wall clock from arrival to read-back of every request"},
+        "gpu_launches": int(launches),
     }
     if pg is not None:
         pg.destroy_process_group()

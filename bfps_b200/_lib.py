@@ -76,6 +76,7 @@ SIGNATURES = {
     "bfg_ens_step": (_i, [_vp, _i]),
     "bfg_ens_last_ms": (_i, [_vp, _pd]),
     "bfg_ens_use_graphs": (_i, [_vp, _i]),
+    "bfg_ens_kernel_launches": (_i, [_vp, _c.POINTER(_i64)]),
 }
 
 _LIB = None

@@ -1548,6 +1548,7 @@ struct EnsGroup {
     size_t cap = 0;
     bfg_ctx launcher;          // stream / SM count / twiddles / errors for this group's launches
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // stage 1 (+ru), 2, 3 + symmetrize
+    int64_t graph_kernels[3] = {0, 0, 0};                       // kernel nodes of each graph
     bool any_tracers = false;
 };
 
@@ -1572,6 +1573,7 @@ struct bfg_ens {
     bool dirty = true;
     bool use_graphs = true;
     int* tctr = nullptr;  // tile counters of the launches on this stream
+    int64_t launches = 0; // kernels launched by bfg_ens_step (graph nodes included)
     std::string err;
 };
 
@@ -1669,6 +1671,9 @@ static int ens_stage(bfg_ens* e, EnsGroup* g, int s) {
 static int ens_prepare(bfg_ens* e) {
     if (!e->dirty) return 0;
     cudaSetDevice(e->device);
+    // nothing in flight may still use the descriptors freed here
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess)
+        return ens_fail(e, BFG_ECUDA, "ensemble stream synchronisation failed");
     ens_free_groups(e);
     std::vector<int> sizes;
     for (auto& en : e->entries)
@@ -1716,7 +1721,9 @@ static int ens_prepare(bfg_ens* e) {
                 cudaGraph_t graph = nullptr;
                 if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
                     return ens_fail(e, BFG_ECUDA, "stream capture failed to start");
+                const int64_t l0 = g->launcher.launches;
                 int rc = ens_stage(e, g, s);
+                g->graph_kernels[s] = g->launcher.launches - l0;
                 cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
                 if (rc || ce != cudaSuccess) {
                     if (graph) cudaGraphDestroy(graph);
@@ -1868,9 +1875,11 @@ int bfg_ens_step(bfg_ens* e, int nsteps) {
         for (auto& en : e->entries)
             if (en.tracers) cudaStreamWaitEvent(e->stream, en.ctx->ev_tr, 0);
         for (EnsGroup* g : e->groups) {
+            const int64_t l0 = g->launcher.launches;
             rc = e->use_graphs ? (cudaGraphLaunch(g->graph[0], e->stream) == cudaSuccess ? 0 : BFG_ECUDA)
                                : ens_stage(e, g, 0);
             if (rc) return ens_fail(e, rc, "stage 1 launch failed");
+            e->launches += e->use_graphs ? g->graph_kernels[0] : g->launcher.launches - l0;
         }
         if (cudaEventRecord(e->ev_ru, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
         if (!e->batched.empty()) {
@@ -1878,6 +1887,7 @@ int bfg_ens_step(bfg_ens* e, int nsteps) {
             rc = e->real_bytes == 4 ? ens_tracers_dispatch<float>(e, p0->neighbours, p0->smoothness)
                                     : ens_tracers_dispatch<double>(e, p0->neighbours, p0->smoothness);
             if (rc) return ens_fail(e, rc, "batched tracer launch failed");
+            e->launches += 2;
             for (int i : e->batched) {
                 // host mirror of tracer_sets_advance
                 bfg_pctx* p = e->entries[i].tracers;
@@ -1890,17 +1900,21 @@ int bfg_ens_step(bfg_ens* e, int nsteps) {
             auto& en = e->entries[i];
             if (!en.tracers) continue;
             bfg_ctx* c = en.ctx;
-            if (std::find(e->batched.begin(), e->batched.end(), i) == e->batched.end() &&
-                (rc = tracer_loop(en.tracers, en.dt, e->stream)))
-                return ens_fail(e, rc, c->err.c_str());
+            if (std::find(e->batched.begin(), e->batched.end(), i) == e->batched.end()) {
+                const int64_t l0 = c->launches;
+                if ((rc = tracer_loop(en.tracers, en.dt, e->stream))) return ens_fail(e, rc, c->err.c_str());
+                e->launches += c->launches - l0;
+            }
             if (cudaEventRecord(c->ev_tr, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
         }
         for (int s = 1; s < 3; ++s)
             for (EnsGroup* g : e->groups) {
+                const int64_t l0 = g->launcher.launches;
                 rc = e->use_graphs
                          ? (cudaGraphLaunch(g->graph[s], e->stream) == cudaSuccess ? 0 : BFG_ECUDA)
                          : ens_stage(e, g, s);
                 if (rc) return ens_fail(e, rc, "stage launch failed");
+                e->launches += e->use_graphs ? g->graph_kernels[s] : g->launcher.launches - l0;
             }
         for (auto& en : e->entries) en.ctx->iteration++;
     }
@@ -1921,6 +1935,12 @@ int bfg_ens_last_ms(bfg_ens* e, double* ms) {
     float f = 0;
     if (cudaEventElapsedTime(&f, e->ev0, e->ev1) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "timing");
     *ms = f;
+    return 0;
+}
+
+int bfg_ens_kernel_launches(const bfg_ens* e, int64_t* count) {
+    if (!e || !count) return BFG_EINVAL;
+    *count = e->launches;
     return 0;
 }
 

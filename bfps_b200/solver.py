@@ -303,6 +303,12 @@ class ensemble:
     def use_graphs(self, enable):
         self._check(lib().bfg_ens_use_graphs(self._h, int(bool(enable))))
 
+    def kernel_launches(self):
+        """Kernels launched by step() so far (graph nodes included)."""
+        n = ctypes.c_int64()
+        self._check(lib().bfg_ens_kernel_launches(self._h, ctypes.byref(n)))
+        return n.value
+
     def close(self):
         if getattr(self, "_h", None):
             lib().bfg_ens_destroy(self._h)

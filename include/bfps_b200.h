@@ -203,6 +203,9 @@ int bfg_ens_step(bfg_ens* e, int nsteps);
 int bfg_ens_last_ms(bfg_ens* e, double* ms);
 /* replay the fluid launches from CUDA graphs (default 1) or launch directly */
 int bfg_ens_use_graphs(bfg_ens* e, int enable);
+/* kernels launched by bfg_ens_step since creation (the nodes of replayed
+ * graphs included) */
+int bfg_ens_kernel_launches(const bfg_ens* e, int64_t* count);
 
 /* ------------------------------------------------------ measurement ---- */
 

@@ -54,6 +54,31 @@ def test_ensemble_equals_alone(graphs):
     ens.close()
 
 
+def test_ensemble_launch_count_same_with_graphs():
+    """The launch counter counts the nodes of replayed graphs: the same
+    kernels are counted with and without graphs, the same number each step."""
+    from bfps_b200.solver import ensemble
+    counts = []
+    for graphs in (True, False):
+        ens = ensemble()
+        ens.use_graphs(graphs)
+        mixed = [_make(s, "single") for s in SPECS]
+        for (ve, ps), s in zip(mixed, SPECS):
+            ens.add(ve, s[6], ps)
+        ens.step(1)
+        one = ens.kernel_launches()
+        ens.step(3)
+        assert ens.kernel_launches() == 4 * one
+        counts.append(one)
+        ens.close()
+        for ve, ps in mixed:
+            if ps is not None:
+                ps.close()
+            ve.close()
+    # three sizes x (5 passes x 3 stages + symmetrize) at least, plus tracers
+    assert counts[0] == counts[1] and counts[0] >= 3 * 16
+
+
 def test_ensemble_member_matches_oracle():
     from bfps_b200.solver import ensemble
     s = SPECS[1]
