@@ -648,7 +648,7 @@ static int ensure_ru(bfg_ctx* c) {
 template <typename T, int NB, int MM>
 static int launch_tracers(bfg_ctx* c, const PParams& pp, bfg_pctx* p, double* out,
                           cudaStream_t st, const void* field) {
-    const unsigned blocks = (unsigned)((p->n + TRACER_THREADS - 1) / TRACER_THREADS);
+    const unsigned blocks = (unsigned)((p->n + tracers_per_block<T>() - 1) / tracers_per_block<T>());
     if (blocks == 0) return 0;
     Prof pr(c, K_TRACER, st);
     tracer_kernel<T, NB, MM><<<blocks, TRACER_THREADS, 0, st>>>(
@@ -1756,7 +1756,8 @@ static int ens_prepare(bfg_ens* e) {
         ts.pos = p->pos;
         ts.hist = p->hist;
         sets.push_back(ts);
-        start.push_back(start.back() + (p->n + TRACER_THREADS - 1) / TRACER_THREADS);
+        const int64_t tpb = e->real_bytes == 4 ? tracers_per_block<float>() : tracers_per_block<double>();
+        start.push_back(start.back() + (p->n + tpb - 1) / tpb);
         e->batched.push_back(i);
     }
     if (!sets.empty()) {

@@ -57,6 +57,12 @@ __device__ __forceinline__ void cell_of(double pos, double box, double h, int N,
     *cell = ((lvl % N) + N) % N;
 }
 
+// periodic index of a stencil point: c in [-N, 2N) (stencils are narrower
+// than the grid), so one conditional add or subtract replaces the modulo
+__device__ __forceinline__ int wrap_once(int c, int N) {
+    return c < 0 ? c + N : (c >= N ? c - N : c);
+}
+
 // x-segment of one stencil row: 2n+2 points x 3 components, contiguous in
 // [z][y][x][c] unless the stencil wraps across the periodic x boundary.
 // Loads 16-byte vectors from the aligned-down start and accumulates
@@ -109,7 +115,7 @@ __device__ __forceinline__ void row_accumulate(const T* __restrict__ row, int x0
     } else {
 #pragma unroll
         for (int ix = 0; ix < NP; ++ix) {
-            const int xx = (x0 + ix + N) % N;
+            const int xx = wrap_once(x0 + ix, N);
             a0 += (double)row[xx * 3 + 0] * wxc[ix];
             a1 += (double)row[xx * 3 + 1] * wxc[ix];
             a2 += (double)row[xx * 3 + 2] * wxc[ix];
@@ -125,23 +131,52 @@ __device__ __forceinline__ void ld_v8(const float* p, float* v) {
                  : "l"(p));
 }
 
-// FP32 field (precision form): the x sums of each stencil row run in FP32
-// with the x weights rounded to FP32; the y/z weights, the accumulation of
-// the row sums and everything after stay FP64.  Three conversions per row
-// instead of one per value.  A row segment is read as 32-byte vectors (one
-// L1 sector each) from its aligned-down start; instead of shifting the loaded
-// words, the x weights are shifted once per tracer (word i of the aligned
-// block belongs to point (i - off) / 3, component (i - off) mod 3) and the
+constexpr int TRACER_THREADS = 128;
+
+// Lanes that share one tracer: two for FP32 fields, one for FP64 fields.  A
+// stencil row is read as up to four (six for n = 5) 32-byte sectors from its
+// aligned-down start.  With one lane per tracer the gather is bound by L1
+// wavefronts (about one per sector, as each lane's sector lies in another
+// line); with the sectors of a row spread over two lanes of one load, a
+// wavefront serves both, and the per-row address and FP64 work only doubles.
+// Measured on B200 (4e6 tracers, n = 3, m = 2, 512^3): 3.26 ms with one lane,
+// 2.70 ms with two, 4.47 ms with four (issue bound).
+template <typename T>
+__host__ __device__ constexpr int tracer_lanes() {
+    return sizeof(T) == 4 ? 2 : 1;
+}
+template <typename T>
+__host__ __device__ constexpr int tracers_per_block() {
+    return TRACER_THREADS / tracer_lanes<T>();
+}
+
+// sum of v over the L lanes of a tracer group, pairwise ((l0 + l1) + (l2 +
+// l3) for four) on every lane (xor partners add the same two values, so all
+// lanes agree)
+template <int L>
+__device__ __forceinline__ double group_sum(double v, unsigned gmask) {
+#pragma unroll
+    for (int m = 1; m < L; m *= 2) v += __shfl_xor_sync(gmask, v, m, L);
+    return v;
+}
+
+// FP32 field (precision form), lane j (0..L-1) of the tracer's group, which
+// reads vectors j, j + L, ... of each row: the x sums of the stencil rows run
+// in FP32 with the x weights rounded to FP32, over the words a lane reads; the
+// y/z weights, the accumulation of those sums over the rows, the sum over the
+// lanes and everything after stay FP64.  Word i of the row segment read from the
+// aligned-down start belongs to point (i - off) / 3, component
+// (i - off) mod 3, so each lane's x weights are shifted once per tracer and its
 // sums are kept per word phase i mod 3, mapped to components at the end.
-template <int NB>
+template <int NB, int L>
 __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int N, const int* g,
                                                int x0, const double* wx, const double* wy,
-                                               const double* wz, double& a0, double& a1,
-                                               double& a2) {
+                                               const double* wz, int j, unsigned gmask,
+                                               double& a0, double& a1, double& a2) {
     constexpr int NP = 2 * NB + 2;
     constexpr int VW = 8;                                // floats per vector
-    constexpr int NV = (3 * NP + 2 * (VW - 1)) / VW;     // vectors covering any alignment
-    constexpr int NF = VW * NV;
+    constexpr int NVMAX = (3 * NP + 2 * (VW - 1)) / VW;  // vectors covering any alignment
+    constexpr int VPL = (NVMAX + L - 1) / L;             // vectors per lane
     const size_t rowN = (size_t)N;
     float wxf[NP];
 #pragma unroll
@@ -150,81 +185,113 @@ __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int
         const int e0 = x0 * 3;
         const int base = e0 & ~(VW - 1);
         const int off = e0 - base;
-        const int maxv = (N * 3 - base) / VW;  // vectors left in the row
-        float wt[NF];
+        // vectors holding stencil words, none past the end of the row
+        const int nv = min((off + 3 * NP + VW - 1) / VW, (N * 3 - base) / VW);
+        float wl[VPL][VW];
 #pragma unroll
-        for (int i = 0; i < NF; ++i) {
-            float w = 0.f;
+        for (int t = 0; t < VPL; ++t)
 #pragma unroll
-            for (int o = 0; o < VW; ++o) {
-                const int k = i - o;
-                if (k >= 0 && k < 3 * NP) w = (off == o) ? wxf[k / 3] : w;
+            for (int u = 0; u < VW; ++u) {
+                const int k = VW * (j + L * t) + u - off;  // 3 * point + component
+                float w = 0.f;
+#pragma unroll
+                for (int pt = 0; pt < NP; ++pt) w = (k >= 3 * pt && k < 3 * pt + 3) ? wxf[pt] : w;
+                wl[t][u] = w;
             }
-            wt[i] = w;
-        }
+        // word u of vector v = j + L t has phase (8 v + u) mod 3, that is
+        // (2 j + 2 L t + u) mod 3: the sums are kept per lane-relative phase
+        // (2 L t + u) mod 3 and rotated by 2 j at the end
         double ph[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
         for (int iz = 0; iz < NP; ++iz) {
-            const int z = (g[2] - NB + iz + N) % N;
+            const int z = wrap_once(g[2] - NB + iz, N);
+            const double bz = wz[iz];
 #pragma unroll 1
             for (int iy = 0; iy < NP; ++iy) {
-                const int y = (g[1] - NB + iy + N) % N;
+                const int y = wrap_once(g[1] - NB + iy, N);
                 const float* row = ru + ((size_t)z * rowN + y) * rowN * 3 + base;
+                const double bzy = bz * wy[iy];
                 float sp[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    if (v < maxv) {
+                for (int t = 0; t < VPL; ++t) {
+                    if (j + L * t < nv) {
                         float q[VW];
-                        ld_v8(row + VW * v, q);
+                        ld_v8(row + VW * (j + L * t), q);
 #pragma unroll
                         for (int u = 0; u < VW; ++u)
-                            sp[(VW * v + u) % 3] = fmaf(q[u], wt[VW * v + u], sp[(VW * v + u) % 3]);
+                            sp[(2 * L * t + u) % 3] = fmaf(q[u], wl[t][u], sp[(2 * L * t + u) % 3]);
                     }
                 }
-                const double bzy = wz[iz] * wy[iy];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) ph[k] = fma(bzy, (double)sp[k], ph[k]);
+                for (int c = 0; c < 3; ++c) ph[c] = fma(bzy, (double)sp[c], ph[c]);
             }
         }
+        // lane-relative phase (k - 2 j) mod 3 holds phase k
+        const int r = (2 * j) % 3;
+        double G[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            G[k] = group_sum<L>(r == 0 ? ph[k] : (r == 1 ? ph[(k + 2) % 3] : ph[(k + 1) % 3]), gmask);
         // component c sits in phase (c + off) mod 3
         const int k0 = off % 3;
-        a0 = k0 == 0 ? ph[0] : (k0 == 1 ? ph[1] : ph[2]);
-        a1 = k0 == 0 ? ph[1] : (k0 == 1 ? ph[2] : ph[0]);
-        a2 = k0 == 0 ? ph[2] : (k0 == 1 ? ph[0] : ph[1]);
+        a0 = k0 == 0 ? G[0] : (k0 == 1 ? G[1] : G[2]);
+        a1 = k0 == 0 ? G[1] : (k0 == 1 ? G[2] : G[0]);
+        a2 = k0 == 0 ? G[2] : (k0 == 1 ? G[0] : G[1]);
     } else {
-        // stencil across the periodic x boundary: scalar loads
+        // stencil across the periodic x boundary: lane j takes the points
+        // ix = j, j + L, ... with scalar loads
+        constexpr int PPL = (NP + L - 1) / L;  // points per lane
+        float wj[PPL];
+        int xj[PPL];
+#pragma unroll
+        for (int m = 0; m < PPL; ++m) {
+            const int ix = j + L * m;
+            float w = 0.f;
+#pragma unroll
+            for (int pt = 0; pt < NP; ++pt) w = ix == pt ? wxf[pt] : w;
+            wj[m] = w;
+            xj[m] = ix < NP ? wrap_once(x0 + ix, N) : -1;
+        }
+        double A[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
         for (int iz = 0; iz < NP; ++iz) {
-            const int z = (g[2] - NB + iz + N) % N;
+            const int z = wrap_once(g[2] - NB + iz, N);
+            const double bz = wz[iz];
 #pragma unroll 1
             for (int iy = 0; iy < NP; ++iy) {
-                const int y = (g[1] - NB + iy + N) % N;
+                const int y = wrap_once(g[1] - NB + iy, N);
                 const float* row = ru + ((size_t)z * rowN + y) * rowN * 3;
                 float s0 = 0.f, s1 = 0.f, s2 = 0.f;
 #pragma unroll
-                for (int ix = 0; ix < NP; ++ix) {
-                    const int xx = (x0 + ix + N) % N;
-                    s0 = fmaf(row[xx * 3 + 0], wxf[ix], s0);
-                    s1 = fmaf(row[xx * 3 + 1], wxf[ix], s1);
-                    s2 = fmaf(row[xx * 3 + 2], wxf[ix], s2);
+                for (int m = 0; m < PPL; ++m) {
+                    if (xj[m] >= 0) {
+                        s0 = fmaf(row[xj[m] * 3 + 0], wj[m], s0);
+                        s1 = fmaf(row[xj[m] * 3 + 1], wj[m], s1);
+                        s2 = fmaf(row[xj[m] * 3 + 2], wj[m], s2);
+                    }
                 }
-                const double bzy = wz[iz] * wy[iy];
-                a0 = fma(bzy, (double)s0, a0);
-                a1 = fma(bzy, (double)s1, a1);
-                a2 = fma(bzy, (double)s2, a2);
+                const double bzy = bz * wy[iy];
+                A[0] = fma(bzy, (double)s0, A[0]);
+                A[1] = fma(bzy, (double)s1, A[1]);
+                A[2] = fma(bzy, (double)s2, A[2]);
             }
         }
+        a0 = group_sum<L>(A[0], gmask);
+        a1 = group_sum<L>(A[1], gmask);
+        a2 = group_sum<L>(A[2], gmask);
     }
 }
 
-constexpr int TRACER_THREADS = 128;
-
-// tracer i of one system: gather u(x_i), then (move) the Adams-Bashforth step
+// tracer i of one system, lane j of its group (tracer_lanes<T>() lanes; gmask
+// the group's lanes): gather u(x_i), then (move) the Adams-Bashforth step.
+// With four lanes, lane d < 3 finishes component d.
 template <typename T, int NB, int MM>
 __device__ __forceinline__ void tracer_one(const PParams& pp, const T* __restrict__ ru,
                                            double* __restrict__ pos, double* __restrict__ hist,
-                                           double* __restrict__ sample_out, int64_t i) {
+                                           double* __restrict__ sample_out, int64_t i, int j,
+                                           unsigned gmask) {
     constexpr int NP = 2 * NB + 2;
+    constexpr int L = tracer_lanes<T>();
     const int N = pp.N;
     double p[3];
     int g[3];
@@ -238,71 +305,70 @@ __device__ __forceinline__ void tracer_one(const PParams& pp, const T* __restric
     beta_weights<NB, MM>(fr[1], wy);
     beta_weights<NB, MM>(fr[2], wz);
 
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    double acc[3] = {0.0, 0.0, 0.0};
     const size_t rowN = (size_t)N;
     const int x0 = g[0] - NB;
     if constexpr (sizeof(T) == 4) {
-        row_gather_f32<NB>(reinterpret_cast<const float*>(ru), N, g, x0, wx, wy, wz, acc0, acc1,
-                           acc2);
+        row_gather_f32<NB, L>(reinterpret_cast<const float*>(ru), N, g, x0, wx, wy, wz, j, gmask,
+                           acc[0], acc[1], acc[2]);
     } else {
 #pragma unroll 1
         for (int iz = 0; iz < NP; ++iz) {
-            const int z = (g[2] - NB + iz + N) % N;
+            const int z = wrap_once(g[2] - NB + iz, N);
 #pragma unroll 1
             for (int iy = 0; iy < NP; ++iy) {
-                const int y = (g[1] - NB + iy + N) % N;
+                const int y = wrap_once(g[1] - NB + iy, N);
                 // coefficient (bz * by) * bx of apply_computation
                 const double bzy = wz[iz] * wy[iy];
                 double wxc[NP];
 #pragma unroll
                 for (int ix = 0; ix < NP; ++ix) wxc[ix] = bzy * wx[ix];
-                row_accumulate<T, NB>(ru + ((size_t)z * rowN + y) * rowN * 3, x0, N, wxc, acc0,
-                                      acc1, acc2);
+                row_accumulate<T, NB>(ru + ((size_t)z * rowN + y) * rowN * 3, x0, N, wxc, acc[0],
+                                      acc[1], acc[2]);
             }
         }
     }
     if (!pp.move) {
-        sample_out[i * 3 + 0] = acc0;
-        sample_out[i * 3 + 1] = acc1;
-        sample_out[i * 3 + 2] = acc2;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (d % L == j) sample_out[i * 3 + d] = acc[d];
         return;
     }
     const int ns = pp.nsteps;
     const size_t slot = (size_t)pp.n * 3;
-    double r0[3] = {acc0, acc1, acc2};
-    double* h0 = hist + (size_t)pp.head * slot + i * 3;
-    if (pp.accum) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) r0[d] += h0[d];
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) h0[d] = r0[d];
-    double r[6][3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) r[0][d] = r0[d];
-    for (int j = 1; j < pp.order; ++j) {
-        const double* hj = hist + (size_t)((pp.head + j) % ns) * slot + i * 3;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) r[j][d] = hj[d];
-    }
     const double dt = pp.dt;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
+        if (d % L != j) continue;
+        double* h0 = hist + (size_t)pp.head * slot + i * 3 + d;
+        double r[6];
+        r[0] = acc[d];
+        if (pp.accum) r[0] += *h0;
+        *h0 = r[0];
+#pragma unroll
+        for (int k = 1; k < 6; ++k) {
+            r[k] = 0.0;
+            if (k < pp.order) {
+                int sl = pp.head + k;
+                sl = sl >= ns ? sl - ns : sl;
+                r[k] = hist[(size_t)sl * slot + i * 3 + d];
+            }
+        }
         double x = p[d];
         switch (pp.order) {
-            case 1: x += dt * r[0][d]; break;
-            case 2: x += dt * (3. * r[0][d] - r[1][d]) / 2.; break;
-            case 3: x += dt * (23. * r[0][d] - 16. * r[1][d] + 5. * r[2][d]) / 12.; break;
+            case 1: x += dt * r[0]; break;
+            case 2: x += dt * (3. * r[0] - r[1]) / 2.; break;
+            case 3: x += dt * (23. * r[0] - 16. * r[1] + 5. * r[2]) / 12.; break;
             case 4:
-                x += dt * (55. * r[0][d] - 59. * r[1][d] + 37. * r[2][d] - 9. * r[3][d]) / 24.;
+                x += dt * (55. * r[0] - 59. * r[1] + 37. * r[2] - 9. * r[3]) / 24.;
                 break;
             case 5:
-                x += dt * (1901. * r[0][d] - 2774. * r[1][d] + 2616. * r[2][d] -
-                           1274. * r[3][d] + 251. * r[4][d]) / 720.;
+                x += dt * (1901. * r[0] - 2774. * r[1] + 2616. * r[2] - 1274. * r[3] +
+                           251. * r[4]) / 720.;
                 break;
             case 6:
-                x += dt * (4277. * r[0][d] - 7923. * r[1][d] + 9982. * r[2][d] -
-                           7298. * r[3][d] + 2877. * r[4][d] - 475. * r[5][d]) / 1440.;
+                x += dt * (4277. * r[0] - 7923. * r[1] + 9982. * r[2] - 7298. * r[3] +
+                           2877. * r[4] - 475. * r[5]) / 1440.;
                 break;
             default: break;
         }
@@ -310,17 +376,25 @@ __device__ __forceinline__ void tracer_one(const PParams& pp, const T* __restric
     }
 }
 
+// lanes of the calling thread's tracer group, as a shuffle mask
+template <int L>
+__device__ __forceinline__ unsigned tracer_group_mask() {
+    const int lane = threadIdx.x & 31;
+    return L == 1 ? (1u << lane) : (((1u << L) - 1u) << (lane & ~(L - 1)));
+}
+
 template <typename T, int NB, int MM>
 __global__ void __launch_bounds__(TRACER_THREADS, 6)
 tracer_kernel(const PParams pp, const T* __restrict__ ru, double* __restrict__ pos,
               double* __restrict__ hist, double* __restrict__ sample_out) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pp.n) return;
-    tracer_one<T, NB, MM>(pp, ru, pos, hist, sample_out, i);
+    constexpr int L = tracer_lanes<T>();
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = t / L;
+    if (i >= pp.n) return;  // whole groups leave together
+    tracer_one<T, NB, MM>(pp, ru, pos, hist, sample_out, i, (int)(t % L), tracer_group_mask<L>());
 }
 
-// the tracer systems of many ensemble members in one launch: thread i
-// belongs to the member k with start[k] <= i < start[k+1]
+// the tracer systems of many ensemble members in one launch
 struct TracerSet {
     PParams pp;     // head, order and accum advance on the device after each loop
     int step_idx;
@@ -344,7 +418,7 @@ __global__ void tracer_sets_advance(TracerSet* __restrict__ sets, int nsets) {
 // bstart[k] <= b < bstart[k+1]; the set is found once per block and its
 // descriptor copied to shared memory.
 template <typename T, int NB, int MM>
-__global__ void __launch_bounds__(TRACER_THREADS)
+__global__ void __launch_bounds__(TRACER_THREADS, 6)
 tracer_batch_kernel(const TracerSet* __restrict__ sets, const int64_t* __restrict__ bstart,
                     int nsets) {
     __shared__ TracerSet s;
@@ -367,9 +441,11 @@ tracer_batch_kernel(const TracerSet* __restrict__ sets, const int64_t* __restric
         for (int w = threadIdx.x; w < (int)(sizeof(TracerSet) / 4); w += blockDim.x) dst[w] = src[w];
     }
     __syncthreads();
-    const int64_t i = ((int64_t)blockIdx.x - bstart[s_k]) * blockDim.x + threadIdx.x;
-    if (i >= s.pp.n) return;
-    tracer_one<T, NB, MM>(s.pp, (const T*)s.ru, s.pos, s.hist, nullptr, i);
+    constexpr int L = tracer_lanes<T>();
+    const int64_t i = ((int64_t)blockIdx.x - bstart[s_k]) * (blockDim.x / L) + threadIdx.x / L;
+    if (i >= s.pp.n) return;  // whole groups leave together
+    tracer_one<T, NB, MM>(s.pp, (const T*)s.ru, s.pos, s.hist, nullptr, i, (int)(threadIdx.x % L),
+                          tracer_group_mask<L>());
 }
 
 // ---------------------------------------------------------------------------
