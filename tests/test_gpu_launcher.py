@@ -1,0 +1,60 @@
+"""The reference's own regression through the launcher.
+
+bfps/test/test_bfps_NSVEparticles.py launches NSVEparticles from the
+fixture's iteration-0 field with its arguments (2 jobs of 32 steps, 10^4
+tracers, checkpoints every 32 steps, statistics every step) and compares
+vorticity/complex, tracers0/state and tracers0/rhs of the run's
+checkpoint file with the fixture at iterations 0, 32 and 64 (max|diff| <
+1e-5).  Here the same launch goes through bfps_b200.dns: the parameter
+file, checkpoints, statistics and tracer samples are written and read with
+bfps_b200.h5, and the run is this package's engine."""
+import numpy as np
+import pytest
+
+from bfps_b200 import h5
+
+pytestmark = pytest.mark.gpu
+
+REF_ARGS = ["NSVEparticles", "-n", "32", "--src-simname", "B32p1e4", "--src-iteration", "0",
+            "--simname", "dns_nsveparticles", "--np", "4", "--ntpp", "1", "--niter_todo", "32",
+            "--niter_out", "32", "--niter_stat", "1", "--checkpoints_per_file", "3",
+            "--nparticles", "10000", "--particle-rand-seed", "2", "--njobs", "2"]
+
+
+def test_reference_regression_through_launcher(tmp_path, golden):
+    from bfps_b200.dns import DNS
+    src = tmp_path / "src"
+    src.mkdir()
+    with h5.File(str(src / "B32p1e4_checkpoint_0.h5"), "w") as f:
+        f["vorticity/complex/0"] = golden["vorticity_0"]
+    c = DNS()
+    c.launch(REF_ARGS + ["--src-wd", str(src), "--wd", str(tmp_path / "run")])
+    nk = golden["state_32"].shape[0]
+    with h5.File(c.get_checkpoint_0_fname()) as f:
+        assert f["vorticity/complex"].keys() == ["0", "32", "64"]
+        for it in (0, 32, 64):
+            assert np.abs(f["vorticity/complex/%d" % it][()] - golden["vorticity_%d" % it]).max() < 1e-5
+        for it in (32, 64):
+            assert np.abs(f["tracers0/state/%d" % it][()][:nk] - golden["state_%d" % it]).max() < 1e-5
+            assert np.abs(f["tracers0/rhs/%d" % it][()][:, :nk] - golden["rhs_%d" % it]).max() < 1e-5
+    with h5.File(c.get_data_file_name()) as f:
+        assert f["iteration"][()] == 64 and f["checkpoint"][()] == 0
+        mom = f["statistics/moments/velocity"][()]
+        spec = f["statistics/spectra/velocity_velocity"][()]
+        hist = f["statistics/histograms/vorticity"][()]
+        assert mom.shape == (65, 10, 4) and spec.shape[0] == 65 and hist.shape == (65, 256, 4)
+        assert np.all(np.isfinite(mom)) and np.all(mom[:, 2, 3] > 0)   # <|u|^2> every step
+        # energy from the spectrum and from the real-space moments agree
+        # (Parseval; the spectrum stops at kM)
+        e_k = 0.5 * (spec[:, :, 0, 0] + spec[:, :, 1, 1] + spec[:, :, 2, 2]).sum(axis=1)
+        assert np.allclose(e_k, 0.5 * mom[:, 2, 3], rtol=0.05)
+        counts = hist.sum(axis=1)[:, :3]
+        assert np.all(counts > 0) and np.all(counts <= 32 ** 3)
+        assert f["kspace/nshell"][()].sum() > 0
+    with h5.File(c.get_particle_file_name()) as f:
+        steps = sorted(int(k) for k in f["tracers0/velocity"].keys())
+        assert steps == list(range(1, 66)) or len(steps) == 65
+        v = f["tracers0/velocity/%d" % steps[0]][()]
+        a = f["tracers0/acceleration/%d" % steps[0]][()]
+        assert v.shape == (1, 10000, 3) and a.shape == (1, 10000, 3)
+        assert np.all(np.isfinite(v)) and np.all(np.isfinite(a)) and np.abs(v).max() > 0
