@@ -169,6 +169,78 @@ class DNS:
     def get_particle_file(self):
         return h5.File(self.get_particle_file_name(), "r")
 
+    # ---------------------------------------------------------- postprocessing
+    def read_parameters(self):
+        """Parameters of an existing run (bfps/_base.py:220-228)."""
+        with self.get_data_file() as f:
+            for k in f["parameters"].keys():
+                if k in self.parameters:
+                    v = f["parameters/" + k][()]
+                    v = v.item() if hasattr(v, "item") else v
+                    v = v.decode() if isinstance(v, bytes) else v
+                    t = type(self.parameters[k])
+                    self.parameters[k] = t(v) if t in (int, float, str) else v
+
+    def compute_statistics(self, iter0=0, iter1=None):
+        """Energy and enstrophy spectra, maximum velocity and energy per
+        statistics step, then the time averages (bfps/DNS.py:196-272); the
+        per-time quantities are kept in `<simname>_postprocess.h5`."""
+        if len(self.statistics) > 0:
+            return
+        self.read_parameters()
+        ns = self.parameters["niter_stat"]
+        with self.get_data_file() as f:
+            if "moments" not in f["statistics"].keys():
+                return
+            mom = f["statistics/moments/velocity"][()]
+            iter0 = min(mom.shape[0] * ns - 1, iter0)
+            last = int(f["iteration"][()])
+            iter1 = last if iter1 is None else min(last, iter1)
+            ii0, ii1 = iter0 // ns, iter1 // ns
+            self.statistics["kshell"] = f["kspace/kshell"][()]
+            self.statistics["kM"] = float(f["kspace/kM"][()])
+            self.statistics["dk"] = float(f["kspace/dk"][()])
+            uu = f["statistics/spectra/velocity_velocity"][()][ii0:ii1 + 1]
+            ww = f["statistics/spectra/vorticity_vorticity"][()][ii0:ii1 + 1]
+        pp = {"iter0": iter0, "iter1": iter1, "ii0": ii0, "ii1": ii1,
+              "t": self.parameters["dt"] * ns * np.arange(ii0, ii1 + 1).astype(np.float64),
+              "energy(t, k)": (uu[:, :, 0, 0] + uu[:, :, 1, 1] + uu[:, :, 2, 2]) / 2,
+              "enstrophy(t, k)": (ww[:, :, 0, 0] + ww[:, :, 1, 1] + ww[:, :, 2, 2]) / 2,
+              "vel_max(t)": mom[ii0:ii1 + 1, 9, 3],
+              "renergy(t)": mom[ii0:ii1 + 1, 2, 3] / 2}
+        name = os.path.join(self.work_dir, self.simname + "_postprocess.h5")
+        with h5.File(name, "w") as f:
+            for k, v in pp.items():
+                f[k] = v
+        for k in ("t", "energy(t, k)", "enstrophy(t, k)", "vel_max(t)", "renergy(t)"):
+            self.statistics[k] = pp[k]
+        self.compute_time_averages()
+
+    def compute_time_averages(self):
+        """Integral and Kolmogorov scales, Reynolds numbers (DNS.py:273-336)."""
+        st, nu = self.statistics, self.parameters["nu"]
+        for key in ("energy", "enstrophy"):
+            st[key + "(t)"] = st["dk"] * np.sum(st[key + "(t, k)"], axis=1)
+        st["Uint(t)"] = np.sqrt(2 * st["energy(t)"] / 3)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            st["Lint(t)"] = ((st["dk"] * np.pi / (2 * st["Uint(t)"] ** 2)) *
+                             np.nansum(st["energy(t, k)"] / st["kshell"][None, :], axis=1))
+        for key in ("energy", "enstrophy", "vel_max", "Uint", "Lint"):
+            if key + "(t)" in st:
+                st[key] = np.average(st[key + "(t)"], axis=0)
+        for sfx in ("", "(t)"):
+            st["diss" + sfx] = nu * st["enstrophy" + sfx] * 2
+            st["etaK" + sfx] = (nu ** 3 / st["diss" + sfx]) ** .25
+            st["tauK" + sfx] = (nu / st["diss" + sfx]) ** .5
+            st["Re" + sfx] = st["Uint" + sfx] * st["Lint" + sfx] / nu
+            st["lambda" + sfx] = (15 * nu * st["Uint" + sfx] ** 2 / st["diss" + sfx]) ** .5
+            st["Rlambda" + sfx] = st["Uint" + sfx] * st["lambda" + sfx] / nu
+            st["kMeta" + sfx] = st["kM"] * st["etaK" + sfx]
+            if self.parameters["dealias_type"] == 1:
+                st["kMeta" + sfx] *= 0.8
+        st["Tint"] = st["Lint"] / st["Uint"]
+        st["Taylor_microscale"] = st["lambda"]
+
     # ---------------------------------------------------------- arguments
     @staticmethod
     def _job_arguments(parser):

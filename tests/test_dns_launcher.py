@@ -232,3 +232,29 @@ def test_job_flow_with_a_stand_in_engine(tmp_path, golden, monkeypatch):
         assert sorted(int(k) for k in f["tracers0/velocity"].keys()) == list(range(1, 18))
         assert f["tracers0/velocity/5"][()].shape == (1, 50, 3)
         assert np.all(f["tracers0/acceleration/5"][()] == -5.0)
+
+
+def test_command_line_and_postprocessing(tmp_path, golden, monkeypatch):
+    """`python -m bfps_b200 DNS ...` (bfps/__main__.py) and
+    DNS.compute_statistics on the run's statistics (DNS.py:196-336)."""
+    from bfps_b200 import solver
+    from bfps_b200.__main__ import main
+    monkeypatch.setattr(solver, "vorticity_equation", _FakeField)
+    monkeypatch.setattr(solver, "particles_system", _FakeTracers)
+    monkeypatch.setattr(solver, "NSVEparticles_step", _fake_step)
+    wd = str(tmp_path / "cli")
+    main(["DNS", "NSVE", "-n", "32", "--simname", "cli", "--niter_todo", "4", "--niter_out", "4",
+          "--niter_stat", "2", "--wd", wd])
+    c = dns.DNS(work_dir=wd, simname="cli")
+    with np.errstate(all="ignore"):   # the stand-in's enstrophy is 0 at t = 0
+        c.compute_statistics()
+    st = c.statistics
+    assert np.allclose(st["t"], c.parameters["dt"] * 2 * np.arange(3))
+    assert np.allclose(st["energy(t, k)"], 1.5 * 2 * np.arange(3)[:, None])
+    assert np.allclose(st["energy(t)"], 1.5 * 2 * np.arange(3) * 17)
+    assert np.allclose(st["renergy(t)"], np.arange(3))
+    assert st["energy"] == pytest.approx(np.mean(1.5 * 2 * np.arange(3) * 17))
+    with h5.File(str(tmp_path / "cli" / "cli_postprocess.h5")) as f:
+        assert f["ii1"][()] == 2 and f["vel_max(t)"].shape == (3,)
+    with pytest.raises(SystemExit):
+        main(["PP"])
