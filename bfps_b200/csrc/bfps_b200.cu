@@ -1550,13 +1550,19 @@ struct EnsGroup {
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // stage 1 (+ru), 2, 3 + symmetrize
     int64_t graph_kernels[3] = {0, 0, 0};                       // kernel nodes of each graph
     bool any_tracers = false;
+    // each size group runs on its own stream, so the passes of small grids
+    // fill the SMs around those of large ones; its own tile counters
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_s1 = nullptr;    // stage 1 (and u(t)) of this step written
+    cudaEvent_t ev_done = nullptr;  // this group's last launch of the call
+    int* tctr = nullptr;
 };
 
 struct bfg_ens {
     int device = 0;
     int real_bytes = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_ru = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_ru = nullptr;  // ev_ru: tracers of the step done
     struct Entry {
         bfg_ctx* ctx;
         bfg_pctx* tracers;
@@ -1572,7 +1578,6 @@ struct bfg_ens {
     int64_t nbatched = 0;       // blocks of the batched tracer launch
     bool dirty = true;
     bool use_graphs = true;
-    int* tctr = nullptr;  // tile counters of the launches on this stream
     int64_t launches = 0; // kernels launched by bfg_ens_step (graph nodes included)
     std::string err;
 };
@@ -1612,9 +1617,14 @@ static void ens_free_groups(bfg_ens* e) {
     e->batched.clear();
     e->nbatched = 0;
     for (EnsGroup* g : e->groups) {
+        if (g->stream) cudaStreamSynchronize(g->stream);
         for (auto& ge : g->graph)
             if (ge) cudaGraphExecDestroy(ge);
         if (g->dmem) cudaFree(g->dmem);
+        if (g->tctr) cudaFree(g->tctr);
+        if (g->ev_s1) cudaEventDestroy(g->ev_s1);
+        if (g->ev_done) cudaEventDestroy(g->ev_done);
+        if (g->stream) cudaStreamDestroy(g->stream);
         delete g;
     }
     e->groups.clear();
@@ -1693,8 +1703,16 @@ static int ens_prepare(bfg_ens* e) {
         g->launcher.real_bytes = c0->real_bytes;
         g->launcher.device = c0->device;
         g->launcher.tw = c0->tw;
-        g->launcher.stream = e->stream;
-        g->launcher.tctr = e->tctr;
+        e->groups.push_back(g);
+        if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&g->ev_s1, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&g->ev_done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMalloc(&g->tctr, 64) != cudaSuccess || cudaMemset(g->tctr, 0, 64) != cudaSuccess) {
+            cudaGetLastError();
+            return ens_fail(e, BFG_ECUDA, "cannot create the group's stream, events or counters");
+        }
+        g->launcher.stream = g->stream;
+        g->launcher.tctr = g->tctr;
         for (int i : g->members) g->any_tracers = g->any_tracers || e->entries[i].tracers != nullptr;
         // member descriptors
         std::vector<unsigned char> host;
@@ -1708,7 +1726,6 @@ static int ens_prepare(bfg_ens* e) {
                 host.insert(host.end(), (unsigned char*)&m, (unsigned char*)&m + sizeof(m));
             }
         }
-        e->groups.push_back(g);
         if (cudaMalloc(&g->dmem, host.size()) != cudaSuccess) {
             cudaGetLastError();
             return ens_fail(e, BFG_ENOMEM, "cannot allocate member descriptors");
@@ -1719,12 +1736,12 @@ static int ens_prepare(bfg_ens* e) {
         if (e->use_graphs) {
             for (int s = 0; s < 3; ++s) {
                 cudaGraph_t graph = nullptr;
-                if (cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+                if (cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess)
                     return ens_fail(e, BFG_ECUDA, "stream capture failed to start");
                 const int64_t l0 = g->launcher.launches;
                 int rc = ens_stage(e, g, s);
                 g->graph_kernels[s] = g->launcher.launches - l0;
-                cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+                cudaError_t ce = cudaStreamEndCapture(g->stream, &graph);
                 if (rc || ce != cudaSuccess) {
                     if (graph) cudaGraphDestroy(graph);
                     return ens_fail(e, rc ? rc : BFG_ECUDA,
@@ -1795,12 +1812,6 @@ int bfg_ens_create(bfg_ens** out, int device) {
     cudaEventCreate(&e->ev0);
     cudaEventCreate(&e->ev1);
     cudaEventCreateWithFlags(&e->ev_ru, cudaEventDisableTiming);
-    if (cudaMalloc(&e->tctr, 64) != cudaSuccess || cudaMemset(e->tctr, 0, 64) != cudaSuccess) {
-        cudaGetLastError();
-        cudaStreamDestroy(e->stream);
-        delete e;
-        return BFG_ENOMEM;
-    }
     *out = e;
     return 0;
 }
@@ -1815,7 +1826,6 @@ void bfg_ens_destroy(bfg_ens* e) {
     cudaEventDestroy(e->ev1);
     cudaEventDestroy(e->ev_ru);
     cudaStreamDestroy(e->stream);
-    if (e->tctr) cudaFree(e->tctr);
     delete e;
 }
 
@@ -1870,19 +1880,31 @@ int bfg_ens_step(bfg_ens* e, int nsteps) {
     cudaSetDevice(e->device);
     int rc = ens_prepare(e);
     if (rc) return rc;
-    if (cudaEventRecord(e->ev0, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
+    // e->stream carries the tracers and orders the call: it starts the
+    // groups (ev0), waits for their stage 1 before the tracers, and joins
+    // them at the end (ev1)
+    for (auto& en : e->entries)
+        if (en.tracers) cudaStreamWaitEvent(e->stream, en.ctx->ev_tr, 0);
+    if (cudaEventRecord(e->ev0, e->stream) != cudaSuccess ||
+        cudaEventRecord(e->ev_ru, e->stream) != cudaSuccess)
+        return ens_fail(e, BFG_ECUDA, "event");
+    auto launch_stage = [&](EnsGroup* g, int s) -> int {
+        const int64_t l0 = g->launcher.launches;
+        int r = e->use_graphs ? (cudaGraphLaunch(g->graph[s], g->stream) == cudaSuccess ? 0 : BFG_ECUDA)
+                              : ens_stage(e, g, s);
+        e->launches += e->use_graphs ? g->graph_kernels[s] : g->launcher.launches - l0;
+        return r;
+    };
     for (int st = 0; st < nsteps; ++st) {
         // the previous step's tracers read ru, which stage 1 rewrites
-        for (auto& en : e->entries)
-            if (en.tracers) cudaStreamWaitEvent(e->stream, en.ctx->ev_tr, 0);
         for (EnsGroup* g : e->groups) {
-            const int64_t l0 = g->launcher.launches;
-            rc = e->use_graphs ? (cudaGraphLaunch(g->graph[0], e->stream) == cudaSuccess ? 0 : BFG_ECUDA)
-                               : ens_stage(e, g, 0);
-            if (rc) return ens_fail(e, rc, "stage 1 launch failed");
-            e->launches += e->use_graphs ? g->graph_kernels[0] : g->launcher.launches - l0;
+            if (cudaStreamWaitEvent(g->stream, e->ev_ru, 0) != cudaSuccess)
+                return ens_fail(e, BFG_ECUDA, "event");
+            if ((rc = launch_stage(g, 0))) return ens_fail(e, rc, "stage 1 launch failed");
+            if (cudaEventRecord(g->ev_s1, g->stream) != cudaSuccess ||
+                cudaStreamWaitEvent(e->stream, g->ev_s1, 0) != cudaSuccess)
+                return ens_fail(e, BFG_ECUDA, "event");
         }
-        if (cudaEventRecord(e->ev_ru, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
         if (!e->batched.empty()) {
             bfg_pctx* p0 = e->entries[e->batched[0]].tracers;
             rc = e->real_bytes == 4 ? ens_tracers_dispatch<float>(e, p0->neighbours, p0->smoothness)
@@ -1908,19 +1930,17 @@ int bfg_ens_step(bfg_ens* e, int nsteps) {
             }
             if (cudaEventRecord(c->ev_tr, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
         }
-        for (int s = 1; s < 3; ++s)
-            for (EnsGroup* g : e->groups) {
-                const int64_t l0 = g->launcher.launches;
-                rc = e->use_graphs
-                         ? (cudaGraphLaunch(g->graph[s], e->stream) == cudaSuccess ? 0 : BFG_ECUDA)
-                         : ens_stage(e, g, s);
-                if (rc) return ens_fail(e, rc, "stage launch failed");
-                e->launches += e->use_graphs ? g->graph_kernels[s] : g->launcher.launches - l0;
-            }
+        if (cudaEventRecord(e->ev_ru, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
+        // stages 2-3 touch neither ru nor the tracer state
+        for (EnsGroup* g : e->groups)
+            for (int s = 1; s < 3; ++s)
+                if ((rc = launch_stage(g, s))) return ens_fail(e, rc, "stage launch failed");
         for (auto& en : e->entries) en.ctx->iteration++;
     }
-    for (auto& en : e->entries)
-        if (en.tracers) cudaStreamWaitEvent(e->stream, en.ctx->ev_tr, 0);
+    for (EnsGroup* g : e->groups)
+        if (cudaEventRecord(g->ev_done, g->stream) != cudaSuccess ||
+            cudaStreamWaitEvent(e->stream, g->ev_done, 0) != cudaSuccess)
+            return ens_fail(e, BFG_ECUDA, "event");
     if (cudaEventRecord(e->ev1, e->stream) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "event");
     // members' own streams follow the ensemble's work
     for (auto& en : e->entries) cudaStreamWaitEvent(en.ctx->stream, e->ev1, 0);
