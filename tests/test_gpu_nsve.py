@@ -112,3 +112,33 @@ def test_beltrami_decays_exactly():
     expect = w * np.exp(-ve.nu * k * k * dt * nsteps)
     assert rel_err(ve.get_cvorticity(), expect) < 1e-12
     ve.close()
+
+
+def test_fp64_anisotropic_box_with_tracers():
+    """dkx != dky != dkz (box lengths 2 pi, 4 pi, pi): k-space tables,
+    dealiasing radius, forcing band and the tracers' box and cell size all
+    follow the per-axis dk (kspace.cpp:34-167, particles_system_builder.hpp:
+    176-179)."""
+    from bfps_b200.solver import vorticity_equation, particles_system, NSVEparticles_step
+    from oracle import particles as P
+    from oracle.nsveparticles import nsveparticles_step
+    n, dk = 32, (1.0, 0.5, 2.0)
+    ve = vorticity_equation(n, n, n, *dk, precision="double")
+    ref = O.VorticityEquation(n, n, n, *dk)
+    for obj in (ve, ref):
+        obj.nu, obj.forcing_type, obj.famplitude, obj.fk0, obj.fk1 = 0.05, "linear", 0.5, 1.5, 3.0
+    w0 = ic.vorticity_ic(n, seed=9)
+    ve.set_cvorticity(w0)
+    ref.cvorticity = w0.copy()
+    rng = np.random.default_rng(9)
+    pos = rng.random((400, 3)) * np.array([2 * np.pi / d for d in dk]) * 1.5 - 1.0
+    ps = particles_system(ve, pos, 2, 1, 3)
+    rps = P.ParticlesSystem(pos, np.zeros((3, 400, 3)), 2, 1, P.Geometry(n, n, n, *dk))
+    for _ in range(3):
+        NSVEparticles_step(ve, ps, 0.005)
+        nsveparticles_step(ref, rps, 0.005)
+    assert rel_err(ve.get_cvorticity(), ref.cvorticity) < 1e-10
+    got, rhs, _ = ps.state()
+    assert rel_err(got, rps.pos) < 1e-10
+    ps.close()
+    ve.close()
