@@ -365,17 +365,20 @@ class File:
         size, _free, data_addr = struct.unpack_from("<QQQ", b, 8)
         return self._rd(data_addr, size)
 
-    def _group_links(self, addr):
+    def _group_links(self, addr, cached=None):
+        """{name: object header address} of a group; names whose entries
+        cache the child group's B-tree and heap (cache type 1) go into
+        `cached` when a set is given."""
         st = self._group_storage(addr)
         if st is None:
             raise H5Error("object at %d is not a group" % addr)
         btree, heap_addr, _ = st
         heap = self._heap(heap_addr)
         links = {}
-        self._walk_group_btree(btree, heap, links)
+        self._walk_group_btree(btree, heap, links, cached)
         return links
 
-    def _walk_group_btree(self, node, heap, links):
+    def _walk_group_btree(self, node, heap, links, cached=None):
         b = self._rd(node, 24)
         if b[:4] != b"TREE" or b[4] != 0:
             raise H5Error("bad group B-tree node at %d" % node)
@@ -384,7 +387,7 @@ class File:
         children = [struct.unpack_from("<Q", body, 8 + 16 * i)[0] for i in range(used)]
         for c in children:
             if level > 0:
-                self._walk_group_btree(c, heap, links)
+                self._walk_group_btree(c, heap, links, cached)
             else:
                 sb = self._rd(c, 8)
                 if sb[:4] != b"SNOD":
@@ -392,9 +395,12 @@ class File:
                 nsym = struct.unpack_from("<H", sb, 6)[0]
                 ents = self._rd(c + 8, 40 * nsym)
                 for i in range(nsym):
-                    noff, oaddr = struct.unpack_from("<QQ", ents, 40 * i)
+                    noff, oaddr, ctype = struct.unpack_from("<QQI", ents, 40 * i)
                     end = heap.index(b"\0", noff)
-                    links[heap[noff:end].decode()] = oaddr
+                    name = heap[noff:end].decode()
+                    links[name] = oaddr
+                    if cached is not None and ctype == 1:
+                        cached.add(name)
 
     def _new_group_storage(self, entries):
         """Write a local heap, one symbol-table node and a one-level B-tree
@@ -433,12 +439,25 @@ class File:
         node += b"\0" * (24 + (2 * 2 * INTERNAL_K + 1) * 8 - len(node))
         return self._append(bytes(node)), heap_addr
 
-    def _set_group_links(self, gaddr, links):
+    def _set_group_links(self, gaddr, links, gpath):
+        """New storage for the group at gpath, pointed to by its symbol-table
+        message.  libhdf5 also caches a group's B-tree and heap addresses in
+        its parent's entry (and the superblock caches the root's): the root
+        cache is rewritten, and a parent whose entry for this group carries a
+        cache gets new storage itself (entries without caches), up the path."""
         btree, heap = self._new_group_storage(list(links.items()))
         _b, _h, body_at = self._group_storage(gaddr)
         self._wr(body_at, struct.pack("<QQ", btree, heap))
         if gaddr == self._root:
             self._wr(self._root_entry_pos + 24, struct.pack("<QQ", btree, heap))
+            return
+        ppath, _, name = gpath.rstrip("/").rpartition("/")
+        ppath = ppath or "/"
+        paddr = self._lookup(ppath)
+        cached = set()
+        plinks = self._group_links(paddr, cached)
+        if name in cached:
+            self._set_group_links(paddr, plinks, ppath)
 
     # ------------------------------------------------------ lookup
     def _lookup(self, path):
@@ -627,6 +646,7 @@ class File:
         addr = self._root
         cur = ""
         for part in [p for p in path.split("/") if p]:
+            parent = cur or "/"
             cur += "/" + part
             links = self._group_links(addr)
             if part in links:
@@ -637,7 +657,7 @@ class File:
                 btree, heap = self._new_group_storage([])
                 new = self._write_object_header([(MSG_STAB, struct.pack("<QQ", btree, heap))])
                 links[part] = new
-                self._set_group_links(addr, links)
+                self._set_group_links(addr, links, parent)
                 addr = new
         return addr
 
@@ -660,7 +680,7 @@ class File:
         if name in links:
             raise H5Error("%s exists" % path)
         links[name] = addr
-        self._set_group_links(paddr, links)
+        self._set_group_links(paddr, links, parent or "/")
 
     @staticmethod
     def _dataspace(shape, maxshape=None):

@@ -118,3 +118,32 @@ def test_rejects_what_it_does_not_read(tmp_path):
     with h5.File(q, "r") as f:
         with pytest.raises(h5.H5Error):
             f["y"] = np.zeros(3)
+
+
+@pytest.mark.skipif(not os.path.exists(FIXTURE), reason="reference checkout absent")
+def test_append_to_reference_written_file(tmp_path, golden):
+    """Adding a checkpoint to a libhdf5-written file: the parent entries that
+    cache a group's B-tree and heap (cache type 1, as libhdf5 writes them)
+    must not keep the old addresses."""
+    import shutil
+    p = str(tmp_path / "cp.h5")
+    shutil.copy(FIXTURE, p)
+    os.chmod(p, 0o644)
+    with h5.File(p) as f:
+        cached = set()
+        f._group_links(f._lookup("/"), cached)
+        assert cached == {"tracers0", "vorticity"}   # libhdf5 caches group entries
+    with h5.File(p, "a") as f:
+        f["vorticity/complex/96"] = golden["vorticity_64"]
+        f["tracers0/state/96"] = np.ones((10, 3))
+    with h5.File(p) as f:
+        assert f["vorticity/complex"].keys() == ["0", "32", "64", "96"]
+        assert np.array_equal(f["vorticity/complex/96"][()], golden["vorticity_64"])
+        assert np.array_equal(f["vorticity/complex/32"][()], golden["vorticity_32"])
+        assert f["tracers0/state"].keys() == ["0", "32", "64", "96"]
+        # every group on the modified paths was rewritten without caches,
+        # so no entry points at the groups' old B-trees and heaps
+        for gpath in ("/", "/vorticity", "/tracers0"):
+            cached = set()
+            f._group_links(f._lookup(gpath), cached)
+            assert cached == set(), gpath
