@@ -77,6 +77,7 @@ SIGNATURES = {
     "bfg_ens_last_ms": (_i, [_vp, _pd]),
     "bfg_ens_use_graphs": (_i, [_vp, _i]),
     "bfg_ens_kernel_launches": (_i, [_vp, _c.POINTER(_i64)]),
+    "bfg_ens_wait": (_i, [_vp, _c.c_double, _c.POINTER(_c.c_int)]),
 }
 
 _LIB = None

@@ -5,12 +5,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -1957,6 +1959,27 @@ int bfg_ens_last_ms(bfg_ens* e, double* ms) {
     if (cudaEventElapsedTime(&f, e->ev0, e->ev1) != cudaSuccess) return ens_fail(e, BFG_ECUDA, "timing");
     *ms = f;
     return 0;
+}
+
+int bfg_ens_wait(bfg_ens* e, double timeout_ms, int* done) {
+    if (!e || !done || !(timeout_ms >= 0.0)) return BFG_EINVAL;
+    cudaSetDevice(e->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(e->ev1);
+        if (q == cudaSuccess) {
+            *done = 1;
+            return 0;
+        }
+        if (q != cudaErrorNotReady) return ens_fail(e, BFG_ECUDA, cudaGetErrorString(q));
+        const double ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms >= timeout_ms) {
+            *done = 0;
+            return 0;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
 }
 
 int bfg_ens_kernel_launches(const bfg_ens* e, int64_t* count) {

@@ -7,7 +7,8 @@ resident on the GPU) and advance together, with the stages of all resident
 requests of the same size batched into one launch per pass.  A tick runs the
 ensemble up to the next event (a resident request reaching its step count,
 or the next arrival as estimated from the measured step time) and
-synchronises once.  A request that reaches its step count is read back and
+synchronises once; while it runs, the host polls it (bfg_ens_wait) and
+prepares the inputs of requests that have arrived.  A request that reaches its step count is read back and
 retired, freeing its memory for waiting requests.  Requests that arrive
 while others are running join at the next tick.
 
@@ -169,6 +170,15 @@ class Server:
                 k = min(k, max(1, int(until * 1e3 / self.step_ms)))
             k = max(1, min(k, self.max_tick))
             self.ens.step(k)
+            # while the tick runs, prepare the inputs of arrived requests
+            # that still need them (host work off the GPU's critical path)
+            while not self.ens.wait(0.002):
+                now = clock() - t0
+                todo = [r for r in waiting + pending[qi:] if r.arrival <= now and r.w0 is None]
+                if not todo:
+                    self.ens.wait()
+                    break
+                prepare(todo[0])
             self.step_ms = self.ens.last_ms() / k
             for rid in list(self.running):
                 self.running[rid][3] += k

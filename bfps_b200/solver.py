@@ -303,6 +303,14 @@ class ensemble:
     def use_graphs(self, enable):
         self._check(lib().bfg_ens_use_graphs(self._h, int(bool(enable))))
 
+    def wait(self, timeout_s=None):
+        """True once the last step() call's work has finished; False if it
+        is still running after timeout_s seconds (None: wait until done)."""
+        done = ctypes.c_int()
+        t = 1e300 if timeout_s is None else max(0.0, timeout_s * 1e3)
+        self._check(lib().bfg_ens_wait(self._h, t, ctypes.byref(done)))
+        return bool(done.value)
+
     def kernel_launches(self):
         """Kernels launched by step() so far (graph nodes included)."""
         n = ctypes.c_int64()

@@ -201,6 +201,11 @@ int bfg_ens_count(const bfg_ens* e, int* members);
 int bfg_ens_step(bfg_ens* e, int nsteps);
 /* device time of the last bfg_ens_step call (synchronises) */
 int bfg_ens_last_ms(bfg_ens* e, double* ms);
+/* poll with a timeout: *done = 1 once the work of the last bfg_ens_step
+ * call has finished, 0 if it is still running after timeout_ms (0 polls
+ * once); the host waits, the device is not blocked.  The serving loop's
+ * "poll with timeout" (bfps' request loop has no counterpart: new) */
+int bfg_ens_wait(bfg_ens* e, double timeout_ms, int* done);
 /* replay the fluid launches from CUDA graphs (default 1) or launch directly */
 int bfg_ens_use_graphs(bfg_ens* e, int enable);
 /* kernels launched by bfg_ens_step since creation (the nodes of replayed

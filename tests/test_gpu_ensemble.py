@@ -79,6 +79,26 @@ def test_ensemble_launch_count_same_with_graphs():
     assert counts[0] == counts[1] and counts[0] >= 3 * 16
 
 
+def test_ensemble_wait_polls_with_timeout():
+    """bfg_ens_wait: a bounded poll of the last step call, then done."""
+    from bfps_b200.solver import ensemble
+    ens = ensemble()
+    mixed = [_make(s, "single") for s in SPECS]
+    for (ve, ps), s in zip(mixed, SPECS):
+        ens.add(ve, s[6], ps)
+    ens.step(200)
+    first = ens.wait(0.0)          # one query, no wait
+    assert first in (True, False)
+    assert ens.wait(None) is True
+    assert ens.wait(0.0) is True
+    assert ens.last_ms() > 0
+    ens.close()
+    for ve, ps in mixed:
+        if ps is not None:
+            ps.close()
+        ve.close()
+
+
 def test_ensemble_member_matches_oracle():
     from bfps_b200.solver import ensemble
     s = SPECS[1]
