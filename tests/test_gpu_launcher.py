@@ -58,3 +58,29 @@ def test_reference_regression_through_launcher(tmp_path, golden):
         a = f["tracers0/acceleration/%d" % steps[0]][()]
         assert v.shape == (1, 10000, 3) and a.shape == (1, 10000, 3)
         assert np.all(np.isfinite(v)) and np.all(np.isfinite(a)) and np.abs(v).max() > 0
+
+
+def test_launcher_fp64_nsve_matches_oracle(tmp_path):
+    """NSVE in double precision from the generated initial field
+    (generate_vector_field): the run's checkpoint matches the FP64 oracle
+    stepped from the same file to 1e-10."""
+    from bfps_b200.dns import DNS
+    from oracle import nsve as O
+    c = DNS()
+    c.launch(["NSVE", "-n", "32", "--precision", "double", "--simname", "d", "--niter_todo", "4",
+              "--niter_out", "4", "--niter_stat", "2", "--wd", str(tmp_path)])
+    p = c.parameters
+    with h5.File(c.get_checkpoint_0_fname()) as f:
+        w0 = f["vorticity/complex/0"][()]
+        w4 = f["vorticity/complex/4"][()]
+    assert w0.dtype == np.complex128
+    ref = O.VorticityEquation(32)
+    ref.nu, ref.forcing_type, ref.famplitude, ref.fk0, ref.fk1 = p["nu"], "linear", p["famplitude"], p["fk0"], p["fk1"]
+    ref.cvorticity = ref.read_checkpoint_semantics(w0)
+    for _ in range(4):
+        ref.step(p["dt"])
+    err = np.abs(w4 - ref.cvorticity).max() / np.abs(ref.cvorticity).max()
+    assert err < 1e-10, err
+    with h5.File(c.get_data_file_name()) as f:
+        assert f["statistics/moments/vorticity"].shape == (3, 10, 4)
+        assert f["iteration"][()] == 4

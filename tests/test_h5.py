@@ -147,3 +147,35 @@ def test_append_to_reference_written_file(tmp_path, golden):
             cached = set()
             f._group_links(f._lookup(gpath), cached)
             assert cached == set(), gpath
+
+
+def test_variable_length_strings(tmp_path):
+    """h5py writes Python str values (bfps_info/*) as variable-length
+    strings in a global heap collection: datatype class 9, elements of
+    (length, collection address, object index)."""
+    import struct
+    p = str(tmp_path / "v.h5")
+    words = [b"linear", b"NSVEparticles-single", b""]
+    with h5.File(p, "w") as f:
+        # a global heap collection holding the strings (objects 1..3)
+        body = b""
+        for i, w in enumerate(words, 1):
+            body += struct.pack("<HH4xQ", i, 1, len(w)) + w + b"\0" * ((-len(w)) % 8)
+        size = 16 + len(body) + 16
+        size = max(size, 4096)
+        coll = b"GCOL" + bytes([1, 0, 0, 0]) + struct.pack("<Q", size) + body
+        coll += struct.pack("<HH4xQ", 0, 0, size - 16 - len(body) - 16) + b"\0" * (size - len(coll) - 16)
+        gaddr = f._append(coll)
+        # a 1-D dataset of three vlen strings: class 9 (version 1), string
+        # type, base type a one-byte unsigned integer
+        base = struct.pack("<B3sI", 0x10, (0).to_bytes(3, "little"), 1) + struct.pack("<HH", 0, 8)
+        dtype = struct.pack("<B3sI", 0x19, (1).to_bytes(3, "little"), 16) + base
+        elems = b"".join(struct.pack("<IQI", len(w), gaddr, i) for i, w in enumerate(words, 1))
+        data = f._append(elems)
+        layout = struct.pack("<BBQQ", 3, 1, data, len(elems))
+        hdr = f._write_object_header([(h5.MSG_DATASPACE, f._dataspace((3,), (3,))),
+                                      (h5.MSG_DATATYPE, dtype, 1), (h5.MSG_LAYOUT, layout, 1)])
+        f._link("/bfps_info/strings", hdr)
+    with h5.File(p) as f:
+        got = f["bfps_info/strings"][()]
+        assert list(got) == ["linear", "NSVEparticles-single", ""]
