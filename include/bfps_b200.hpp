@@ -8,6 +8,8 @@
  *                                            (bfps/cpp/particles/abstract_particles_system.hpp:12-55)
  *   bfps_b200::NSVEparticles_step            NSVEparticles::step
  *                                            (bfps/cpp/full_code/NSVEparticles.cpp:33-41)
+ *   bfps_b200::ensemble                      batched form over bfg_ens_* (no
+ *                                            counterpart in the reference)
  *
  * The public physical members (nu, fmode, famplitude, fk0, fk1,
  * forcing_type) are plain data as in the reference and are read whenever a
@@ -19,11 +21,15 @@
 #ifndef BFPS_B200_HPP
 #define BFPS_B200_HPP
 
+#include <algorithm>
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <stdexcept>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "bfps_b200.h"
 
@@ -208,6 +214,66 @@ inline void NSVEparticles_step(vorticity_equation<rnumber>& fs, particles_system
           "NSVEparticles_step");
     fs.pull_iteration();
 }
+
+/* Members of any sizes advanced together, one launch per pass and RK stage
+ * for each grid size; a member keeps its state and API but is stepped only
+ * through the ensemble while it belongs to it. */
+class ensemble {
+  public:
+    explicit ensemble(int device = 0) {
+        if (bfg_ens_create(&e, device) != BFG_OK) throw error("bfg_ens_create", BFG_ECUDA);
+    }
+    ~ensemble() { bfg_ens_destroy(e); }
+    ensemble(const ensemble&) = delete;
+    ensemble& operator=(const ensemble&) = delete;
+
+    template <typename rnumber>
+    void add(vorticity_equation<rnumber>& fs, double dt, particles_system* ps = nullptr) {
+        fs.push_physics();
+        chk(bfg_ens_add(e, fs.handle(), ps ? ps->handle() : nullptr, dt), "ensemble::add");
+        members.emplace_back(fs.handle(), [&fs] { fs.pull_iteration(); });
+    }
+    template <typename rnumber>
+    void remove(vorticity_equation<rnumber>& fs) {
+        chk(bfg_ens_remove(e, fs.handle()), "ensemble::remove");
+        members.erase(std::remove_if(members.begin(), members.end(),
+                                     [&fs](const auto& m) { return m.first == fs.handle(); }),
+                      members.end());
+    }
+    /* nsteps NSVEparticles steps of every member (enqueued; the members'
+     * iteration counters advance at once) */
+    void step(int nsteps) {
+        chk(bfg_ens_step(e, nsteps), "ensemble::step");
+        for (auto& m : members) m.second();
+    }
+    /* true once the last step() has finished, false if still running after
+     * timeout_ms */
+    bool wait(double timeout_ms) {
+        int done = 0;
+        chk(bfg_ens_wait(e, timeout_ms, &done), "ensemble::wait");
+        return done != 0;
+    }
+    double last_ms() {
+        double ms = 0;
+        chk(bfg_ens_last_ms(e, &ms), "ensemble::last_ms");
+        return ms;
+    }
+    int count() const {
+        int n = 0;
+        chk(bfg_ens_count(e, &n), "ensemble::count");
+        return n;
+    }
+
+  private:
+    void chk(int rc, const char* what) const {
+        if (rc != BFG_OK)
+            throw error(std::string(what) + ": " + bfg_ens_last_error(e) + " (code " +
+                            std::to_string(rc) + ")",
+                        rc);
+    }
+    bfg_ens* e = nullptr;
+    std::vector<std::pair<bfg_ctx*, std::function<void()>>> members;
+};
 
 }  // namespace bfps_b200
 

@@ -1,8 +1,8 @@
 """The C++ mirror (include/bfps_b200.hpp) of vorticity_equation,
 particles_system and NSVEparticles::step: it compiles against the C-ABI, and
 a C++ program driving it the way NSVEparticles does gives bit for bit the
-results of the same calls through the Python mirror, and the oracle's to
-1e-10 in FP64."""
+results of the same calls through the Python mirror (also when the steps go
+through a one-member C++ ensemble), and the oracle's to 1e-10 in FP64."""
 import os
 import shutil
 import subprocess
@@ -30,8 +30,9 @@ def test_cpp_mirror_compiles_and_links(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["double", "single"])
-def test_cpp_driver_matches_python_mirror_and_oracle(tmp_path, precision):
+@pytest.mark.parametrize("precision,mode", [("double", "alone"), ("single", "alone"),
+                                            ("single", "ensemble")])
+def test_cpp_driver_matches_python_mirror_and_oracle(tmp_path, precision, mode):
     from bfps_b200 import ic
     from bfps_b200.solver import vorticity_equation, particles_system, NSVEparticles_step
     from oracle import nsve as O
@@ -49,7 +50,8 @@ def test_cpp_driver_matches_python_mirror_and_oracle(tmp_path, precision):
     with open(fin, "wb") as f:
         f.write(np.ascontiguousarray(w0).tobytes())
         f.write(np.ascontiguousarray(pos).tobytes())
-    subprocess.check_call([exe, str(rb), str(n), str(nt), str(steps), repr(dt), fin, fout])
+    subprocess.check_call([exe, str(rb), str(n), str(nt), str(steps), repr(dt), fin, fout] +
+                          (["ensemble"] if mode == "ensemble" else []))
     raw = open(fout, "rb").read()
     it, sidx = np.frombuffer(raw[:8], np.int32)
     off = 8
