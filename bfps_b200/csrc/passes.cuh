@@ -104,7 +104,11 @@ template <typename T, int NB>
 __host__ __device__ constexpr int col_pitch_for(int tkx) {
     return NB * 3 * tkx + (sizeof(T) == 4 ? 2 : 1);
 }
-// number of RK operand arrays streamed with the tile (FZ passes)
+// number of RK operand arrays the FZ epilogue reads (v0, and v_prev for
+// stages 2-3).  They are read from global memory after an L2 prefetch at
+// the start of the tile, not staged in shared memory: staging them took the
+// shared memory of a tile twice as wide (4 instead of 8 kx columns at 512^3
+// FP32), and the wider tile measured 19 % faster (2.42 -> 1.97 ms).
 __host__ __device__ constexpr int col_nrk(int mode) {
     return mode == CM_FZ_RK1 ? 1 : ((mode == CM_FZ_RK2 || mode == CM_FZ_RK3) ? 2 : 0);
 }
@@ -114,12 +118,10 @@ __host__ __device__ constexpr int col_nrk(int mode) {
 // and loads are covered by the other CTA's work (measured faster for IZ,
 // slower for IY and FY).  Otherwise one 512-thread CTA per SM with two tile
 // buffers, the next tile loading while this one is transformed.
-// shared memory: nbuf tile buffers + the RK operand tile + twiddles
+// shared memory: nbuf tile buffers + twiddles
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t col_bytes_nb(int tkx, int nbuf) {
-    return (size_t)(nbuf * N * col_pitch_for<T, col_nb(MODE)>(tkx) + col_nrk(MODE) * N * 3 * tkx +
-                    N) *
-           sizeof(cpx<T>);
+    return (size_t)(nbuf * N * col_pitch_for<T, col_nb(MODE)>(tkx) + N) * sizeof(cpx<T>);
 }
 // kx columns per tile: the widest power of two (<= 16) within the budget
 template <typename T, int N, int MODE>
@@ -436,8 +438,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     constexpr int NRK = col_nrk(MODE);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* bufs = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* rkt = bufs + NBUF * TILE;     // RK operand tile [arr][l][W] (FZ passes)
-    cpx<T>* tw = rkt + NRK * N * W;
+    cpx<T>* tw = bufs + NBUF * TILE;
 
     constexpr int NXV = N / 2 + 1;
     constexpr size_t nxp3 = (size_t)(N / 2 + 4) * 3;
@@ -474,24 +475,23 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             for (int i = tid; i < NWORDS; i += NT) dst[i] = src[i];
         }
         if constexpr (NRK > 0) {
-            // RK operands of this tile: rows S[ky=a][kz=l], streamed while the
-            // tile is transformed (the epilogue of the previous tile is done)
+            // RK operands of this tile, rows S[ky=a][kz=l][kx0..kx0+TKX): into
+            // L2 while the tile is transformed, read by the epilogue
             const int a = tl / ntx;
             const int kx0 = (tl % ntx) * TKX;
             const cpx<T>* rk_v0 = mbuf(mem[m], rl.v0);  // mb is not yet visible to all
-            const cpx<T>* rk_vp = mbuf(mem[m], rl.vp);
-            const int nvalid = (3 * min(TKX, NXV - kx0) + VPE - 1) / VPE;
-            for (int e = tid; e < N * NRK * WV; e += NT) {
-                const int v = e % WV;
-                const int r = e / WV;
+            const cpx<T>* rk_vp = NRK > 1 ? mbuf(mem[m], rl.vp) : rk_v0;
+            constexpr int LINES = (3 * TKX * (int)sizeof(cpx<T>) + 127) / 128 + 1;
+            const int nbytes = 3 * min(TKX, NXV - kx0) * (int)sizeof(cpx<T>);
+            for (int e = tid; e < N * NRK * LINES; e += NT) {
+                const int q = e % LINES;
+                const int r = e / LINES;
                 const int arr = r % NRK;
                 const int l = r / NRK;
-                if (v >= nvalid) continue;
-                const cpx<T>* src = ((arr == 0) ? rk_v0 : rk_vp) + ((size_t)a * N + l) * nxp3 +
-                                    (size_t)kx0 * 3 + v * VPE;
-                cp_async<VB>(&rkt[(arr * N + l) * W + v * VPE], src);
+                const char* row = reinterpret_cast<const char*>(
+                    ((arr == 0) ? rk_v0 : rk_vp) + ((size_t)a * N + l) * nxp3 + (size_t)kx0 * 3);
+                if (128 * q < nbytes) prefetch_l2(row + 128 * q);
             }
-            cp_async_commit();
         }
         if constexpr (NBUF == 2) {
             // the next tile streams into the other buffer while this one is transformed
@@ -505,8 +505,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             }
             cp_async_commit();
         }
-        if constexpr (NRK > 0) cp_async_wait<2>();
-        else if constexpr (NBUF == 2) cp_async_wait<1>();
+        if constexpr (NBUF == 2) cp_async_wait<1>();
         else cp_async_wait<0>();
         __syncthreads();
         // ticket for the tile after the prefetched one (two buffers) or for
@@ -571,14 +570,13 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
             if (ncol == TKX) dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, NT);
             else dif<T, N, INV, PN, LYN, 1, N>(tile, tw, tid, NT);
-            cp_async_wait<1>();  // RK operand tile of this tile
             __syncthreads();
             // ---- epilogue: one thread per mode (kz = l, kx = kx0 + col)
             const double ky = kwrap<N>(a, kp.dky);
             auto mode = [&](int col, int l, const FzCol<T>& fc) {
                 const size_t pt = ((size_t)a * N + l) * (N / 2 + 4) + kx0 + col;  // S[ky=a][kz=l][kx]
-                const cpx<T>* v0 = &rkt[l * W + col * 3];
-                const cpx<T>* vp = &rkt[((NRK - 1) * N + l) * W + col * 3];
+                const cpx<T>* v0 = mbuf(mb, rl.v0) + pt * 3;
+                const cpx<T>* vp = NRK > 1 ? mbuf(mb, rl.vp) + pt * 3 : v0;
                 fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, fc, v0, vp, pt, mb.filt,
                                      mb.fac, mbuf(mb, rl.fsrc), mbuf(mb, rl.out0));
             };
