@@ -118,3 +118,27 @@ def test_fp32_field_sample_error_bound(n, nm):
     assert err < 2e-6, err
     ps.close()
     ve.close()
+
+
+def test_zero_tracers():
+    """An empty tracer system: the step is the fluid step alone, the state
+    arrays are empty, sampling returns nothing."""
+    from bfps_b200.solver import vorticity_equation, particles_system, NSVEparticles_step
+    n = 32
+    w0 = ic.vorticity_ic(n, seed=21)
+    out = []
+    for with_ps in (True, False):
+        ve = vorticity_equation(n, precision="double")
+        ve.nu, ve.forcing_type = 0.05, "linear"
+        ve.set_cvorticity(w0)
+        ps = particles_system(ve, np.zeros((0, 3)), 2, 1, 3) if with_ps else None
+        NSVEparticles_step(ve, ps, 0.01, 3)
+        out.append(ve.get_cvorticity())
+        if ps is not None:
+            pos, rhs, idx = ps.state()
+            assert pos.shape == (0, 3) and rhs.shape == (3, 0, 3) and idx.shape == (0,)
+            assert ps.sample_velocity().shape == (0, 3)
+            assert ps.step_idx == 4
+            ps.close()
+        ve.close()
+    assert np.array_equal(out[0], out[1])
