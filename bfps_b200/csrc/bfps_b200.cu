@@ -692,7 +692,7 @@ static PParams pparams(const bfg_pctx* p, double dt, int move) {
     return pp;
 }
 
-// counting sort of the tracers by (z, y) cell row (tracer_keys / bucket_scan /
+// counting sort of the tracers by (z, y) cell row (tracer_keys / bucket scans /
 // tracer_scatter); swaps the state arrays with their second copies
 static int tracer_sort(bfg_pctx* p, cudaStream_t st = nullptr) {
     bfg_ctx* c = p->ctx;
@@ -706,8 +706,15 @@ static int tracer_sort(bfg_pctx* p, cudaStream_t st = nullptr) {
     tracer_keys<<<blocks, 256, 0, st>>>(pp, p->pos, p->key, p->rank, p->count);
     int rc = after_launch(c, "tracer_keys");
     if (rc) return rc;
-    bucket_scan<<<1, 1024, 0, st>>>(p->count, p->offset, nb);
-    if ((rc = after_launch(c, "bucket_scan"))) return rc;
+    // offset holds nb bucket offsets followed by up to 1024 block sums
+    const int nblk = (nb + 1023) / 1024;
+    unsigned* bsum = p->offset + nb;
+    bucket_block_sums<<<nblk, 1024, 0, st>>>(p->count, bsum, nb);
+    if ((rc = after_launch(c, "bucket_block_sums"))) return rc;
+    bucket_scan_sums<<<1, 1024, 0, st>>>(bsum, nblk);
+    if ((rc = after_launch(c, "bucket_scan_sums"))) return rc;
+    bucket_scan_blocks<<<nblk, 1024, 0, st>>>(p->count, bsum, p->offset, nb);
+    if ((rc = after_launch(c, "bucket_scan_blocks"))) return rc;
     tracer_scatter<<<blocks, 256, 0, st>>>(pp, p->key, p->rank, p->offset, p->pos, p->hist,
                                             p->corder, p->pos2, p->hist2, p->corder2);
     if ((rc = after_launch(c, "tracer_scatter"))) return rc;
@@ -1228,7 +1235,8 @@ int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, 
               cudaMalloc(&p->sample, nb) == cudaSuccess &&
               cudaMalloc(&p->key, n1 * 4) == cudaSuccess &&
               cudaMalloc(&p->rank, n1 * 4) == cudaSuccess &&
-              cudaMalloc(&p->count, nbk) == cudaSuccess && cudaMalloc(&p->offset, nbk) == cudaSuccess;
+              cudaMalloc(&p->count, nbk) == cudaSuccess &&
+              cudaMalloc(&p->offset, nbk + 1024 * sizeof(unsigned)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         bfg_particles_destroy(p);

@@ -482,28 +482,59 @@ __global__ void tracer_keys(const PParams pp, const double* __restrict__ pos,
     rank[i] = atomicAdd(&count[k], 1u);
 }
 
-// exclusive scan of nb counts with one CTA of 1024 threads
-__global__ void __launch_bounds__(1024) bucket_scan(const unsigned* __restrict__ count,
-                                                    unsigned* __restrict__ offset, int nb) {
-    __shared__ unsigned part[1024];
-    const int t = threadIdx.x;
-    const int per = (nb + 1023) / 1024;
-    const int b0 = t * per, b1 = min(nb, b0 + per);
-    unsigned s = 0;
-    for (int b = b0; b < b1; ++b) s += count[b];
-    part[t] = s;
+// Exclusive scan of the nb bucket counts in three launches: the sum of each
+// 1024-bucket block, an exclusive scan of those sums (one CTA: nb <= 2^20,
+// i.e. N <= 1024), then each block's own scan plus its block offset.
+// Integer sums, so the offsets do not depend on the order of the additions.
+// 1024 threads per CTA; returns v's exclusive prefix within the CTA and the
+// CTA's total in *total.
+__device__ __forceinline__ unsigned cta_scan_1024(unsigned v, unsigned* ws, unsigned* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[warp] = x;
     __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        const unsigned v = t >= o ? part[t - o] : 0u;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    if (warp == 0) {
+        unsigned w = ws[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        ws[lane] = w;  // inclusive over the warps
     }
-    unsigned run = part[t] - s;  // exclusive prefix of this thread's range
-    for (int b = b0; b < b1; ++b) {
-        offset[b] = run;
-        run += count[b];
-    }
+    __syncthreads();
+    *total = ws[31];
+    return (warp == 0 ? 0u : ws[warp - 1]) + x - v;
+}
+__global__ void __launch_bounds__(1024) bucket_block_sums(const unsigned* __restrict__ count,
+                                                          unsigned* __restrict__ bsum, int nb) {
+    __shared__ unsigned ws[32];
+    const int i = blockIdx.x * 1024 + threadIdx.x;
+    unsigned total;
+    cta_scan_1024(i < nb ? count[i] : 0u, ws, &total);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+__global__ void __launch_bounds__(1024) bucket_scan_sums(unsigned* __restrict__ bsum, int nblk) {
+    __shared__ unsigned ws[32];
+    const int t = threadIdx.x;
+    const unsigned v = t < nblk ? bsum[t] : 0u;
+    unsigned total;
+    const unsigned ex = cta_scan_1024(v, ws, &total);  // every read precedes the barriers
+    if (t < nblk) bsum[t] = ex;
+}
+__global__ void __launch_bounds__(1024) bucket_scan_blocks(const unsigned* __restrict__ count,
+                                                           const unsigned* __restrict__ bsum,
+                                                           unsigned* __restrict__ offset, int nb) {
+    __shared__ unsigned ws[32];
+    const int i = blockIdx.x * 1024 + threadIdx.x;
+    unsigned total;
+    const unsigned ex = cta_scan_1024(i < nb ? count[i] : 0u, ws, &total);
+    if (i < nb) offset[i] = bsum[blockIdx.x] + ex;
 }
 
 __global__ void tracer_scatter(const PParams pp, const unsigned* __restrict__ key,

@@ -142,3 +142,30 @@ def test_zero_tracers():
             ps.close()
         ve.close()
     assert np.array_equal(out[0], out[1])
+
+
+def test_cell_sort_over_many_bucket_blocks():
+    """64^3: 4096 (z, y) buckets, scanned in four 1024-bucket blocks; the
+    sorted tracers come back in index order unchanged and step as the
+    oracle's."""
+    from bfps_b200.solver import vorticity_equation, particles_system, NSVEparticles_step
+    n = 64
+    ve = vorticity_equation(n, precision="double")
+    ref = O.VorticityEquation(n)
+    for obj in (ve, ref):
+        obj.nu, obj.forcing_type, obj.famplitude, obj.fk0, obj.fk1 = 0.02, "linear", 0.5, 1.5, 3.0
+    w0 = ic.vorticity_ic(n, seed=31)
+    ve.set_cvorticity(w0)
+    ref.cvorticity = w0.copy()
+    pos = ic.tracer_ic(5000, seed=32)
+    ps = particles_system(ve, pos, 2, 1, 3)
+    p0, r0, i0 = ps.state()
+    assert np.array_equal(p0, pos) and np.array_equal(i0, np.arange(5000)) and not r0.any()
+    rps = P.ParticlesSystem(pos, np.zeros((3, 5000, 3)), 2, 1, P.Geometry(n, n, n))
+    for _ in range(2):
+        NSVEparticles_step(ve, ps, 0.004)
+        nsveparticles_step(ref, rps, 0.004)
+    got, _, _ = ps.state()
+    assert rel_err(got, rps.pos) < 1e-10
+    ps.close()
+    ve.close()
