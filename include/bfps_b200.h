@@ -38,7 +38,7 @@ typedef struct bfg_pctx bfg_pctx;
 #define BFG_EINVAL -1     /* bad argument */
 #define BFG_ECUDA -2      /* CUDA runtime error */
 #define BFG_ENOMEM -3     /* device allocation failed */
-#define BFG_EUNSUP -4     /* configuration not supported by this build */
+#define BFG_EUNSUP -4     /* configuration the library does not support */
 #define BFG_ESTATE -5     /* call not valid in the current state */
 
 /* dealiasing (bfps/cpp/kspace.hpp:40, enum kspace_dealias_type) */

@@ -9,8 +9,8 @@ where they lie in the reference checkout and writes one shared library,
 exact-rational restatement in ``oracle/interp.py`` (and through it the
 coefficient header used by the CUDA gather kernel).
 
-No reference source is copied; if the checkout is absent (as on a GPU box)
-the build is skipped and a previously built library is used if present.
+No reference source is copied; where the checkout is absent the build is
+skipped and a previously built library is used if present.
 """
 import os
 import subprocess

@@ -1,7 +1,7 @@
 """IF-RK3 vorticity step on the GPU against the FP64 oracle.
 
-Gate: FP64 fields agree to 1e-10 relative over the
-first 8 steps.
+Gate: FP64 fields agree with the oracle to 1e-10 relative over the first 8
+steps.
 """
 import numpy as np
 import pytest
