@@ -1230,29 +1230,38 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         }
         __syncthreads();
         if constexpr (WRITE_RU) {
-            // real u (u pencils after the inverse transform) in natural x order
-            // 16-byte vectors of the (contiguous) output rows
+            // real u (u pencils after the inverse transform) in natural x
+            // order: complex word posn[j] of component c's pencil holds
+            // u(2j, c) and u(2j+1, c), so a thread takes four x (two words
+            // per component) and writes their 12 values [x][c] as 16-byte
+            // vectors of the (contiguous) output row
             T* rout = mreal(mem[m], rl.rout) + row0 * (N * 3);
-            const T* PT = reinterpret_cast<const T*>(P);
-            constexpr int VR = 16 / (int)sizeof(T);
-            constexpr int RV = N * 3 / VR;  // vectors per row
-            for (int v = tid; v < ROWS * RV; v += RNL_THREADS) {
-                const int r = v / RV;
-                const int e0 = (v - r * RV) * VR;
-                T val[VR];
+            constexpr int QR = N / 4;  // four-x groups per row
+            for (int v = tid; v < ROWS * QR; v += RNL_THREADS) {
+                const int r = v / QR;
+                const int k = v - r * QR;
+                const int p0 = posn[2 * k], p1 = posn[2 * k + 1];
+                T val[12];
 #pragma unroll
-                for (int i = 0; i < VR; ++i) {
-                    const int e = e0 + i;
-                    const int xx = e / 3;
-                    const int c = e - 3 * xx;
-                    val[i] = PT[2 * (r * RG + c * PL + posn[xx >> 1]) + (xx & 1)];
+                for (int c = 0; c < 3; ++c) {
+                    const cpx<T> lo = P[r * RG + c * PL + p0];
+                    const cpx<T> hi = P[r * RG + c * PL + p1];
+                    val[c] = lo.x;
+                    val[3 + c] = lo.y;
+                    val[6 + c] = hi.x;
+                    val[9 + c] = hi.y;
                 }
-                if constexpr (VR == 4)
-                    *reinterpret_cast<float4*>(rout + r * (N * 3) + e0) =
-                        make_float4(val[0], val[1], val[2], val[3]);
-                else
-                    *reinterpret_cast<double2*>(rout + r * (N * 3) + e0) =
-                        make_double2(val[0], val[1]);
+                T* dst = rout + (size_t)r * (N * 3) + (size_t)k * 12;
+                if constexpr (sizeof(T) == 4) {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+                        reinterpret_cast<float4*>(dst)[q] =
+                            make_float4(val[4 * q], val[4 * q + 1], val[4 * q + 2], val[4 * q + 3]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 6; ++q)
+                        reinterpret_cast<double2*>(dst)[q] = make_double2(val[2 * q], val[2 * q + 1]);
+                }
             }
             if constexpr (NS == 2) __syncthreads();  // phase E overwrites the u pencils
         }
