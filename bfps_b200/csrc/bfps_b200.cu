@@ -99,6 +99,7 @@ struct bfg_pctx {
     unsigned* rank = nullptr;
     unsigned* count = nullptr;
     unsigned* offset = nullptr;
+    unsigned* perm = nullptr;   // source of each cell-order slot during a sort
     int resort_every = 4;    // 0: never (grids below 256^3 keep u in L2 anyway)
     int loops_since_sort = 0;
     std::vector<int64_t> idx;       // global index of each tracer, creation order
@@ -693,7 +694,7 @@ static PParams pparams(const bfg_pctx* p, double dt, int move) {
 }
 
 // counting sort of the tracers by (z, y) cell row (tracer_keys / bucket scans /
-// tracer_scatter); swaps the state arrays with their second copies
+// tracer_perm / tracer_gather); swaps the state arrays with their second copies
 static int tracer_sort(bfg_pctx* p, cudaStream_t st = nullptr) {
     bfg_ctx* c = p->ctx;
     if (!st) st = c->stream;
@@ -715,9 +716,11 @@ static int tracer_sort(bfg_pctx* p, cudaStream_t st = nullptr) {
     if ((rc = after_launch(c, "bucket_scan_sums"))) return rc;
     bucket_scan_blocks<<<nblk, 1024, 0, st>>>(p->count, bsum, p->offset, nb);
     if ((rc = after_launch(c, "bucket_scan_blocks"))) return rc;
-    tracer_scatter<<<blocks, 256, 0, st>>>(pp, p->key, p->rank, p->offset, p->pos, p->hist,
-                                            p->corder, p->pos2, p->hist2, p->corder2);
-    if ((rc = after_launch(c, "tracer_scatter"))) return rc;
+    tracer_perm<<<blocks, 256, 0, st>>>(pp, p->key, p->rank, p->offset, p->perm);
+    if ((rc = after_launch(c, "tracer_perm"))) return rc;
+    tracer_gather<<<blocks, 256, 0, st>>>(pp, p->perm, p->pos, p->hist, p->corder, p->pos2,
+                                           p->hist2, p->corder2);
+    if ((rc = after_launch(c, "tracer_gather"))) return rc;
     std::swap(p->pos, p->pos2);
     std::swap(p->hist, p->hist2);
     std::swap(p->corder, p->corder2);
@@ -1235,6 +1238,7 @@ int bfg_particles_create(bfg_ctx* c, bfg_pctx** out, int64_t n, int neighbours, 
               cudaMalloc(&p->sample, nb) == cudaSuccess &&
               cudaMalloc(&p->key, n1 * 4) == cudaSuccess &&
               cudaMalloc(&p->rank, n1 * 4) == cudaSuccess &&
+              cudaMalloc(&p->perm, n1 * 4) == cudaSuccess &&
               cudaMalloc(&p->count, nbk) == cudaSuccess &&
               cudaMalloc(&p->offset, nbk + 1024 * sizeof(unsigned)) == cudaSuccess;
     if (!ok) {
@@ -1271,7 +1275,7 @@ void bfg_particles_destroy(bfg_pctx* p) {
         cudaStreamSynchronize(p->ctx->stream);
     }
     void* bufs[] = {p->pos, p->pos2, p->hist, p->hist2, p->corder, p->corder2,
-                    p->sample, p->key, p->rank, p->count, p->offset};
+                    p->sample, p->key, p->rank, p->count, p->offset, p->perm};
     for (void* b : bufs)
         if (b) cudaFree(b);
     delete p;

@@ -537,15 +537,26 @@ __global__ void __launch_bounds__(1024) bucket_scan_blocks(const unsigned* __res
     if (i < nb) offset[i] = bsum[blockIdx.x] + ex;
 }
 
-__global__ void tracer_scatter(const PParams pp, const unsigned* __restrict__ key,
-                               const unsigned* __restrict__ rank,
-                               const unsigned* __restrict__ offset,
-                               const double* __restrict__ pos, const double* __restrict__ hist,
-                               const int64_t* __restrict__ idx, double* __restrict__ pos2,
-                               double* __restrict__ hist2, int64_t* __restrict__ idx2) {
+// The tracers in cell order.  tracer_perm records the source of every
+// destination (src[offset[key] + rank] = i, one 4-byte store per tracer);
+// tracer_gather then copies positions, rhs history and indexes with the
+// writes in order and the reads at random (random partial-sector writes,
+// as a direct scatter makes them, cost a read-modify-write each).
+__global__ void tracer_perm(const PParams pp, const unsigned* __restrict__ key,
+                            const unsigned* __restrict__ rank, const unsigned* __restrict__ offset,
+                            unsigned* __restrict__ src) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= pp.n) return;
-    const int64_t d = (int64_t)offset[key[i]] + rank[i];
+    src[offset[key[i]] + rank[i]] = (unsigned)i;
+}
+
+__global__ void tracer_gather(const PParams pp, const unsigned* __restrict__ src,
+                              const double* __restrict__ pos, const double* __restrict__ hist,
+                              const int64_t* __restrict__ idx, double* __restrict__ pos2,
+                              double* __restrict__ hist2, int64_t* __restrict__ idx2) {
+    const int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= pp.n) return;
+    const int64_t i = src[d];
     const size_t slot = (size_t)pp.n * 3;
 #pragma unroll
     for (int c = 0; c < 3; ++c) pos2[d * 3 + c] = pos[i * 3 + c];
