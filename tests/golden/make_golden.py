@@ -3,10 +3,9 @@
 Source: bfps/test/B32p1e4_checkpoint_0.h5, the fixture of the reference's
 only asserting regression test (bfps/test/test_bfps_NSVEparticles.py:12-52):
 NSVEparticles, N=32, single precision, 10^4 tracers with beta_n1_m1, AB4,
-run as two jobs of 32 steps.  libhdf5/h5py are not available, so the file is
-decoded directly: every dataset is contiguous (HDF5 superblock v0) and is
-read at its data offset; each offset is validated by content (the IC
-positions equal ``np.random.seed(2); np.random.random((10000,3))*2*pi``
+run as two jobs of 32 steps.  libhdf5/h5py are not available; the file is
+read through its groups by bfps_b200.h5, and the contents are checked (the
+IC positions equal ``np.random.seed(2); np.random.random((10000,3))*2*pi``
 bit for bit, the shifted rhs[0] is zero, the fields are Hermitian on the
 kx=0 plane at iterations 32 and 64, which were written after symmetrize).
 
@@ -17,20 +16,16 @@ import os
 import sys
 import numpy as np
 
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from bfps_b200 import h5  # noqa: E402
+
 SRC = "/root/reference/bfps/test/B32p1e4_checkpoint_0.h5"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "B32p1e4.npz")
 
-# dataset -> (byte offset of the contiguous data, dtype, shape)
-DATASETS = {
-    "vorticity/complex/0": (3520, np.complex64, (32, 32, 17, 3)),
-    "vorticity/complex/32": (667000, np.complex64, (32, 32, 17, 3)),
-    "vorticity/complex/64": (2288888, np.complex64, (32, 32, 17, 3)),
-    "tracers0/state/0": (424952, "<f8", (10000, 3)),
-    "tracers0/state/32": (1086840, "<f8", (10000, 3)),
-    "tracers0/state/64": (2708728, "<f8", (10000, 3)),
-    "tracers0/rhs/32": (1326840, "<f8", (4, 10000, 3)),
-    "tracers0/rhs/64": (2948728, "<f8", (4, 10000, 3)),
-}
+DATASETS = ["vorticity/complex/0", "vorticity/complex/32", "vorticity/complex/64",
+            "tracers0/state/0", "tracers0/state/32", "tracers0/state/64",
+            "tracers0/rhs/32", "tracers0/rhs/64"]
 
 # number of tracers kept in the committed fixture (tracers are independent
 # given the field, so a prefix is an exact sub-check of the full comparison)
@@ -38,14 +33,8 @@ NKEEP = 2000
 
 
 def read_all(path=SRC):
-    raw = open(path, "rb").read()
-    if raw[:8] != b"\x89HDF\r\n\x1a\n":
-        raise ValueError("not an HDF5 file")
-    out = {}
-    for name, (off, dt, shape) in DATASETS.items():
-        n = int(np.prod(shape)) * np.dtype(dt).itemsize
-        out[name] = np.frombuffer(raw[off:off + n], dtype=dt).reshape(shape).copy()
-    return out
+    with h5.File(path, "r") as f:
+        return {name: f[name][()] for name in DATASETS}
 
 
 def validate(d):
