@@ -258,3 +258,15 @@ def test_command_line_and_postprocessing(tmp_path, golden, monkeypatch):
         assert f["ii1"][()] == 2 and f["vel_max(t)"].shape == (3,)
     with pytest.raises(SystemExit):
         main(["PP"])
+
+
+def test_generated_field_equals_the_reference_generator():
+    """The launcher's initial field equals the reference's own
+    generate_data_3D + padd_with_zeros run (tests/golden/make_ic_golden.py),
+    bit for bit."""
+    ref = np.load(os.path.join(os.path.dirname(__file__), "golden", "ic_vector_field_n16.npz"))["field"]
+    c = NoRun()
+    c.prepare_launch(["NSVE", "-n", "16"])
+    got = c.generate_vector_field(spectra_slope=2.0, amplitude=0.05)
+    assert got.dtype == ref.dtype and got.shape == ref.shape == (16, 16, 9, 3)
+    assert np.array_equal(got, ref)
