@@ -142,3 +142,24 @@ def test_fp64_anisotropic_box_with_tracers():
     assert rel_err(got, rps.pos) < 1e-10
     ps.close()
     ve.close()
+
+
+def test_fp64_kolmogorov_with_tracers():
+    """Kolmogorov forcing (mode fmode = 2) with tracers on the C3
+    interpolation kernel (n = 3, m = 2), AB3, three NSVEparticles steps."""
+    from bfps_b200.solver import particles_system, NSVEparticles_step
+    from oracle import particles as P
+    from oracle.nsveparticles import nsveparticles_step
+    ve, ref = _pair(32, O.SMOOTH, "Kolmogorov", seed=4)
+    pos = ic.tracer_ic(700, seed=44)
+    ps = particles_system(ve, pos, 3, 2, 3)
+    rps = P.ParticlesSystem(pos, np.zeros((3, 700, 3)), 3, 2, P.Geometry(32, 32, 32))
+    for _ in range(3):
+        NSVEparticles_step(ve, ps, 0.01)
+        nsveparticles_step(ref, rps, 0.01)
+    assert rel_err(ve.get_cvorticity(), ref.cvorticity) < 1e-10
+    got, rhs, _ = ps.state()
+    assert rel_err(got, rps.pos) < 1e-10
+    assert rel_err(rhs[1], rps.rhs[1]) < 1e-10
+    ps.close()
+    ve.close()

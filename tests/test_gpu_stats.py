@@ -31,3 +31,30 @@ def test_stats_match_oracle():
     spec_u = got["velocity"][0]
     assert abs(0.5 * np.trace(spec_u, axis1=1, axis2=2).sum() - 0.5) < 1e-12
     ve.close()
+
+
+@pytest.mark.parametrize("dealias", [O.SMOOTH, O.TWO_THIRDS])
+def test_stats_anisotropic_box(dealias):
+    """Spectra, moments and histograms with dkx != dky != dkz and both
+    dealiasing rules: shells keyed by |k| / min(dk), kM from the largest
+    axis bound (kspace.cpp:75-150, 521-598)."""
+    from bfps_b200.solver import vorticity_equation
+    n, dk = 32, (1.0, 0.5, 2.0)
+    ve = vorticity_equation(n, n, n, *dk, precision="double", dealias_type=dealias)
+    w0 = ic.vorticity_ic(n, seed=7)
+    ve.set_cvorticity(w0)
+    ref = O.VorticityEquation(n, n, n, *dk, dealias_type=dealias)
+    ref.cvorticity = w0.copy()
+    ks = ve.kspace()
+    assert ks["nshells"] == ref.kk.nshells
+    assert np.allclose(ks["kshell"], ref.kk.kshell, rtol=1e-13)
+    assert np.array_equal(ks["nshell"], ref.kk.nshell)
+    got = ve.do_stats(1.0, 5.0, 64)
+    want = O.nsve_do_stats(ref, 1.0, 5.0, 64)
+    for name in ("velocity", "vorticity"):
+        gs, gm, gh = got[name]
+        ws, wm, wh = want[name]
+        assert rel_err(gs, ws) < 1e-12
+        assert np.abs(gm - wm).max() <= 1e-10 * np.abs(wm).max()
+        assert np.abs(gh - wh).sum() <= 4 and gh.sum() == wh.sum()
+    ve.close()
