@@ -1491,23 +1491,58 @@ moments_pitched_kernel(const T* __restrict__ r, int nx, int pitch, size_t npts, 
         if (shist_p[i]) atomicAdd(&hist[i], (unsigned long long)shist_p[i]);
 }
 
-// Device address of g_noalloc_partials on the current device.  Host code
-// cannot use the array's name as a device pointer, so the address is looked
-// up once per device (cudaGetSymbolAddress, with that device current) and
-// cached; the lookup happens inside the first call made on each device.
+// Device address of g_noalloc_partials in the current device context.  Host
+// code cannot use the array's name as a device pointer, so the address is
+// looked up (cudaGetSymbolAddress, with the device current) and cached per
+// device context: the key is the context's unique id (cuCtxGetId, reached
+// through cudaGetDriverEntryPoint so that nothing links libcuda), so a
+// device reset, which creates a new context and may load the module at a new
+// address, makes the next call look the address up again.  Where the context
+// id cannot be read the address is looked up on every call.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+static bool current_ctx_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (CtxGetCurrentFn)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)f;
+        cudaGetLastError();
+    }
+    if (!get_cur || !get_id) return false;
+    void* ctx = nullptr;
+    if (get_cur(&ctx) != 0 || !ctx) return false;
+    return get_id(ctx, id) == 0;
+}
+
 static double* noalloc_partials_on(int device, cudaError_t* err) {
     static std::mutex mu;
-    static std::unordered_map<int, double*> addr;
+    static std::unordered_map<unsigned long long, double*> addr;  // context id -> address
     std::lock_guard<std::mutex> lk(mu);
-    auto it = addr.find(device);
-    if (it != addr.end()) return it->second;
+    unsigned long long id = 0;
+    const bool keyed = current_ctx_id(&id);
+    if (keyed) {
+        auto it = addr.find(id);
+        if (it != addr.end()) return it->second;
+    }
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess) {
+        cudaGetLastError();  // do not leave the lookup's error pending
         *err = e;
         return nullptr;
     }
-    addr[device] = static_cast<double*>(p);
+    (void)device;
+    if (keyed) addr[id] = static_cast<double*>(p);
     return static_cast<double*>(p);
 }
 
@@ -1528,6 +1563,9 @@ extern "C" int bfg_rspace_stats_noalloc(const void* dev_field, int nx, int ny, i
     if (!partials) return BFG_ECUDA;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t npts = (size_t)nx * ny * nz;
+    // the reference's padded real layout: rows of 2 (nx/2 + 1) points
+    // (field_layout of the in-place R2C buffer), nx + 2 for even nx
+    const int pitch = 2 * (nx / 2 + 1);
     // the histogram is accumulated into the caller's output: start it at zero
     if (cudaMemsetAsync(dev_hist, 0, (size_t)nbins * 4 * sizeof(int64_t), s) != cudaSuccess) {
         cudaGetLastError();
@@ -1537,12 +1575,14 @@ extern "C" int bfg_rspace_stats_noalloc(const void* dev_field, int nx, int ny, i
     const size_t shmem = (size_t)nbins * 4 * sizeof(unsigned int);
     if (real_bytes == 4)
         moments_pitched_kernel<float><<<STATS_BLOCKS, STATS_THREADS, shmem, s>>>(
-            static_cast<const float*>(dev_field), nx, nx + 2, npts, max_estimate, max_estimate,
+            static_cast<const float*>(dev_field), nx, pitch, npts, max_estimate, max_estimate,
             max_estimate, me3, nbins, partials, reinterpret_cast<unsigned long long*>(dev_hist));
     else
         moments_pitched_kernel<double><<<STATS_BLOCKS, STATS_THREADS, shmem, s>>>(
-            static_cast<const double*>(dev_field), nx, nx + 2, npts, max_estimate, max_estimate,
+            static_cast<const double*>(dev_field), nx, pitch, npts, max_estimate, max_estimate,
             max_estimate, me3, nbins, partials, reinterpret_cast<unsigned long long*>(dev_hist));
+    // a failed first launch must not queue the final reduction
+    if (cudaGetLastError() != cudaSuccess) return BFG_ECUDA;
     moments_final<<<1, 64, 0, s>>>(partials, STATS_BLOCKS, 1.0 / (double)npts, dev_moments);
     if (cudaGetLastError() != cudaSuccess) return BFG_ECUDA;
     return BFG_OK;

@@ -250,9 +250,11 @@ int bfg_kernel_launches(const bfg_ctx* ctx, int64_t* count);
  *
  * Allocates nothing: the per-block partial sums live in a fixed 370 KiB
  * device array inside the library, present on every GPU that loads it until
- * the library is unloaded.  The first call on a device looks up that
+ * the library is unloaded.  The first call in each device context (and the
+ * first after a device reset, which creates a new context) looks up that
  * array's device address (with the device current) and should come before
- * any stream capture.  All calls share the array, so calls that overlap on
+ * any stream capture.  Rows are 2 (nx/2 + 1) values apart (nx + 2 for even
+ * nx).  All calls share the array, so calls that overlap on
  * the GPU (for example on two streams at once) race; order them.  The
  * histogram output is cleared by the call itself.  nbins above
  * BFG_NOALLOC_MAX_BINS returns BFG_EUNSUP. */

@@ -99,12 +99,28 @@ class KSpace:
                          minlength=self.nshells)[:self.nshells]
         self.kshell = np.where(self.nshell != 0, ks / np.maximum(self.nshell, 1), 0.0)
         if dealias_type == SMOOTH:
-            # table keyed by round(k2/dk2) (kspace.cpp:135); with equal dk per
-            # axis every key maps to a single k2, so the direct formula is the
-            # same table lookup.
-            self.filter = np.exp(-36.0 * np.power(k2 / self.kM2, 18.0))
+            # the reference keeps one filter value per key round(k2/dk2)
+            # (kspace.cpp:119-150); where several k2 share a key (incommensurate
+            # dk per axis) the entry written last in CLOOP order (y, z, x;
+            # kspace.hpp:117-192) wins, as with one OpenMP thread.  Every mode
+            # is then multiplied by the entry of its own key (kspace.cpp:479).
+            keys = np.rint(k2 / self.dk2).astype(np.int64)  # round half to even
+            # round() of the reference rounds halves away from zero
+            half = np.abs(k2 / self.dk2 - np.floor(k2 / self.dk2) - 0.5) == 0
+            keys = np.where(half, np.floor(k2 / self.dk2).astype(np.int64) + 1, keys)
+            vals = np.exp(-36.0 * np.power(k2 / self.kM2, 18.0))
+            flat_k = keys.reshape(-1)   # C order = CLOOP order (y, z, x)
+            flat_v = vals.reshape(-1)
+            table = np.zeros(int(flat_k.max()) + 1)
+            # last occurrence of each key in CLOOP order
+            rev = flat_k[::-1]
+            uk, first_in_rev = np.unique(rev, return_index=True)
+            table[uk] = flat_v[::-1][first_in_rev]
+            self.filter_table = table
+            self.filter = table[keys]
         else:
             self.filter = None
+            self.filter_table = None
 
     # -- pointwise k-space operations ------------------------------------
     def dealias(self, a):

@@ -1,6 +1,7 @@
 """The reference arm of bench.py (`--impl reference`) on the host: one JSON
-line with the bench contract's keys, timed on the CPU restatement (the C1
-workload, so that it runs in seconds)."""
+line with the bench contract's keys, timed on the C++/OpenMP restatement
+(the C1 workload, so that it runs in seconds); `steps` is the number of whole
+steps actually timed (at least three, at most K)."""
 import json
 import os
 import subprocess
@@ -22,6 +23,7 @@ def test_reference_arm_prints_one_contract_line():
               "impl", "cpu_baseline", "e2e"):
         assert k in d, k
     assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "steps/s"
+    assert 2 <= d["steps"] <= 2 and d["warmup"] == 1
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
