@@ -60,6 +60,7 @@ struct bfg_ctx {
     std::vector<unsigned char> hmember;  // last uploaded copy
     void* stats_ws = nullptr;  // statistics partial sums
     int* tctr = nullptr;       // tile counters of the persistent passes (self-resetting)
+    unsigned long long* dcount = nullptr;  // bfg_check_finite's counter
     size_t stats_ws_bytes = 0;
     size_t field_bytes = 0;
     cudaStream_t stream = nullptr;
@@ -780,7 +781,7 @@ void bfg_ctx_destroy(bfg_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     void* bufs[] = {c->w0, c->v1, c->v2, c->wa, c->wb, c->ru, c->tw, c->filt, c->fac, c->stats_ws,
-                    c->dmember, c->tctr};
+                    c->dmember, c->tctr, c->dcount};
     for (void* b : bufs)
         if (b) cudaFree(b);
     for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
@@ -1163,6 +1164,37 @@ int bfg_stats(bfg_ctx* c, double max_velocity_estimate, double max_vorticity_est
     if ((rc = dispatch<OpStats>(c, (int)B_WA, max_velocity_estimate / std::sqrt(3.0),
                                 nbins, spec_vel, mom_vel, hist_vel)))
         return rc;
+    return 0;
+}
+
+int bfg_check_finite(bfg_ctx* c, int field_id, int64_t* nonfinite) {
+    if (!c || !nonfinite) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    const void* dev;
+    size_t nvals;
+    if (field_id == BFG_FIELD_VORTICITY || field_id == BFG_FIELD_VELOCITY) {
+        dev = field_id == BFG_FIELD_VORTICITY ? c->w0 : c->wa;
+        nvals = (size_t)c->n * c->n * c->nxp * 3 * 2;  // padding columns hold zeros
+    } else if (field_id == BFG_FIELD_RVELOCITY) {
+        if (int rc = ensure_ru(c)) return rc;
+        dev = c->ru;
+        nvals = (size_t)c->n * c->n * c->n * 3;
+    } else {
+        return fail(c, BFG_EINVAL, "unknown field id %d", field_id);
+    }
+    if (!c->dcount) CU(cudaMalloc(&c->dcount, sizeof(unsigned long long)));
+    CU(cudaMemsetAsync(c->dcount, 0, sizeof(unsigned long long), c->stream));
+    if (c->real_bytes == 4)
+        nonfinite_kernel<float><<<c->nsm * 8, 256, 0, c->stream>>>((const float*)dev, nvals, c->dcount);
+    else
+        nonfinite_kernel<double><<<c->nsm * 8, 256, 0, c->stream>>>((const double*)dev, nvals,
+                                                                   c->dcount);
+    if (int rc = after_launch(c, "nonfinite")) return rc;
+    unsigned long long h = 0;
+    CU(cudaMemcpyAsync(&h, c->dcount, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    *nonfinite = (int64_t)h;
     return 0;
 }
 

@@ -8,8 +8,14 @@ template <typename T, int N>
 int Engine<T, N>::stats(bfg_ctx* c, int cfield, double max_est, int nbins, double* spec,
                         double* mom, int64_t* hist) {
     const size_t spec_n = (size_t)c->nshells * 9;
-    const size_t need = spec_n * 8 + (size_t)STATS_BLOCKS * NQ * 8 + NQ * 8 +
-                        (size_t)nbins * 4 * 8;
+    // spectrum: SPEC_BLOCKS partials of spec_n doubles, then the result
+    int spec_warps = SPEC_WARPS_MAX;
+    while (spec_warps > 1 && (size_t)spec_warps * spec_n * 8 > (size_t)c->smem_optin) --spec_warps;
+    if (spec_n * 8 > (size_t)c->smem_optin)
+        return fail(c, BFG_EUNSUP, "%d shells do not fit the spectrum kernel's shared memory",
+                    c->nshells);
+    const size_t need = spec_n * 8 + (size_t)SPEC_BLOCKS * spec_n * 8 +
+                        (size_t)STATS_BLOCKS * NQ * 8 + NQ * 8 + (size_t)nbins * 4 * 8;
     if (c->stats_ws_bytes < need) {
         if (c->stats_ws) cudaFree(c->stats_ws);
         c->stats_ws = nullptr;
@@ -18,18 +24,23 @@ int Engine<T, N>::stats(bfg_ctx* c, int cfield, double max_est, int nbins, doubl
         c->stats_ws_bytes = need;
     }
     double* d_spec = (double*)c->stats_ws;
-    double* d_part = d_spec + spec_n;
+    double* d_spart = d_spec + spec_n;
+    double* d_part = d_spart + (size_t)SPEC_BLOCKS * spec_n;
     double* d_mom = d_part + (size_t)STATS_BLOCKS * NQ;
     unsigned long long* d_hist = (unsigned long long*)(d_mom + NQ);
-    CU(cudaMemsetAsync(d_spec, 0, spec_n * 8, c->stream));
     CU(cudaMemsetAsync(d_hist, 0, (size_t)nbins * 4 * 8, c->stream));
     const KParams kp = kparams(c, 0.0);
     Prof pr0(c, K_STATS);
     const void* cptr = cfield == B_W0 ? c->w0 : c->wa;
-    spectrum_kernel<T, N><<<STATS_BLOCKS, 256, spec_n * 8, c->stream>>>(
-        kp, (const C*)cptr, c->nshells, c->dk, d_spec);
+    const size_t spec_smem = (size_t)spec_warps * spec_n * 8;
+    CU(ensure_smem(spectrum_kernel<T, N>, spec_smem, c->device));
+    spectrum_kernel<T, N><<<SPEC_BLOCKS, spec_warps * 32, spec_smem, c->stream>>>(
+        kp, (const C*)cptr, c->nshells, c->dk, d_spart);
     int rc = after_launch(c, "spectrum");
     if (rc) return rc;
+    spectrum_final<<<(unsigned)((spec_n + 255) / 256), 256, 0, c->stream>>>(d_spart, SPEC_BLOCKS,
+                                                                          (int)spec_n, d_spec);
+    if ((rc = after_launch(c, "spectrum_final"))) return rc;
     // real-space field into v2 (as [z][y][x][3] reals)
     if ((rc = col<CM_IZ_PLAIN>(c, self(c), 1, roles(cfield, B_NONE, B_WB, B_NONE)))) return rc;
     if ((rc = col<CM_Y_INV1>(c, self(c), 1, roles(B_WB, B_NONE, B_WB, B_NONE)))) return rc;

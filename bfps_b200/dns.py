@@ -569,18 +569,40 @@ class _Job:
         return self.dns.get_checkpoint_fname(self.checkpoint)
 
     # direct_numerical_simulation::main_loop
+    # (direct_numerical_simulation.cpp:89-118): stats, step, checkpoint every
+    # niter_out, then the stopping condition, every iteration
     def main_loop(self):
         p = self.p
         it = self.iteration
         max_iter = it + p["niter_todo"] - (it % p["niter_todo"])
+        self.stopped = False
         while self.iteration < max_iter:
             self.do_stats()
             self.step()
             if self.iteration % p["niter_out"] == 0:
                 self.write_checkpoint()
+            if self.check_stopping_condition():
+                self.stopped = True
+                break
         self.do_stats()
         if self.iteration % p["niter_out"] != 0:
             self.write_checkpoint()
+
+    # code_base::check_stopping_condition (code_base.cpp:15-35): a file
+    # named stop_<simname> in the run's working directory ends the loop
+    def check_stopping_condition(self):
+        return os.path.exists(os.path.join(self.dns.work_dir, "stop_" + self.dns.simname))
+
+    # The reference traps floating-point exceptions in its host arithmetic
+    # (main_code.hpp:48-52); the arithmetic here runs on the device, so the
+    # state is scanned on the device before statistics and checkpoints are
+    # written, and a non-finite value stops the run with an error instead of
+    # a corrupted file.
+    def check_finite(self):
+        bad = self.fs.count_nonfinite("vorticity")
+        if bad:
+            raise FloatingPointError("iteration %d: %d non-finite values in the vorticity field"
+                                     % (self.iteration, bad))
 
     def step(self):
         from .solver import NSVEparticles_step
@@ -594,6 +616,7 @@ class _Job:
     def do_stats(self):
         p = self.p
         if self.iteration % p["niter_stat"] == 0:
+            self.check_finite()
             st = self.fs.do_stats(p["max_velocity_estimate"], p["max_vorticity_estimate"],
                                   p["histogram_bins"])
             t = self.iteration // p["niter_stat"]
@@ -633,6 +656,7 @@ class _Job:
     def write_checkpoint(self):
         if not self.output:
             return
+        self.check_finite()
         self._update_checkpoint()
         fname = self._fname()
         with h5.File(fname, "a") as f:

@@ -124,8 +124,13 @@ class Server:
     def _finish(self, rid, now):
         req, fs, ps, _ = self.running.pop(rid)
         self.ens.remove(fs)
+        # the final state's statistics (NSVE::do_stats): the energy spectrum
+        # E(k) = tr(spec_uu) / 2, summed in a fixed order on the device, so a
+        # request gives the same bits alone and in the mix
+        spec_uu = fs.do_stats()["velocity"][0]
         req.result = {"vorticity_checksum": float(np.abs(fs.get_cvorticity()).sum()),
-                      "iteration": fs.iteration}
+                      "iteration": fs.iteration,
+                      "energy_spectrum": 0.5 * np.einsum("kii->k", spec_uu)}
         if ps is not None:
             req.result["tracers"] = ps.state()[0]
             ps.close()

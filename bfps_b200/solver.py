@@ -173,6 +173,15 @@ class vorticity_equation:
         check(lib().bfg_lagrangian_acceleration(self._h, out.ctypes.data), self._h)
         return out
 
+    def count_nonfinite(self, field="vorticity"):
+        """Number of NaN / Inf values in a field on the device
+        (bfg_check_finite)."""
+        fid = {"vorticity": _lib.FIELD_VORTICITY, "velocity": _lib.FIELD_VELOCITY,
+               "rvelocity": _lib.FIELD_RVELOCITY}[field]
+        n = ctypes.c_int64()
+        check(lib().bfg_check_finite(self._h, fid, ctypes.byref(n)), self._h)
+        return n.value
+
     def last_step_ms(self):
         ms = ctypes.c_double()
         check(lib().bfg_last_step_ms(self._h, ctypes.byref(ms)), self._h)

@@ -135,6 +135,14 @@ int bfg_stats(bfg_ctx* ctx, double max_velocity_estimate, double max_vorticity_e
               int nbins, double* spec_vel, double* spec_vort, double* mom_vel,
               double* mom_vort, int64_t* hist_vel, int64_t* hist_vort);
 
+/* Number of non-finite values (NaN or +-Inf, real and imaginary parts
+ * counted separately) in a field on the device, written to *nonfinite.
+ * Stands in for the floating-point-exception trapping the reference enables
+ * in its host code (bfps/cpp/full_code/main_code.hpp:48-52), which cannot
+ * see device arithmetic: a run checks its state with it and stops instead
+ * of writing a corrupted checkpoint.  field_id as for bfg_field_download. */
+int bfg_check_finite(bfg_ctx* ctx, int field_id, int64_t* nonfinite);
+
 /* ---------------------------------------------------------- tracers ---- */
 
 /* particles_system_builder (bfps/cpp/particles/particles_system_builder.hpp:

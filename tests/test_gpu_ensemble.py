@@ -163,6 +163,9 @@ def test_serving_results_equal_alone():
         NSVEparticles_step(fs, ps, r.dt, r.steps)
         assert r.result["iteration"] == r.steps
         assert r.result["vorticity_checksum"] == float(np.abs(fs.get_cvorticity()).sum())
+        # statistics too, bit for bit (fixed-order spectrum reduction)
+        spec_alone = 0.5 * np.einsum("kii->k", fs.do_stats()["velocity"][0])
+        assert np.array_equal(r.result["energy_spectrum"], spec_alone)
         if ps is not None:
             assert np.array_equal(r.result["tracers"], ps.state()[0])
         assert r.finished >= r.admitted >= r.arrival

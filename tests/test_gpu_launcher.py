@@ -84,3 +84,54 @@ def test_launcher_fp64_nsve_matches_oracle(tmp_path):
     with h5.File(c.get_data_file_name()) as f:
         assert f["statistics/moments/vorticity"].shape == (3, 10, 4)
         assert f["iteration"][()] == 4
+
+
+def test_launcher_stop_file_ends_the_loop(tmp_path):
+    """A file stop_<simname> in the working directory ends main_loop after
+    the current iteration (code_base.cpp:15-35, checked every iteration by
+    direct_numerical_simulation.cpp:108-110); the final statistics and
+    checkpoint follow."""
+    from bfps_b200.dns import DNS
+    wd = tmp_path / "run"
+    wd.mkdir()
+    (wd / "stop_s").write_text("")
+    c = DNS()
+    c.launch(["NSVE", "-n", "16", "--simname", "s", "--niter_todo", "8", "--niter_out", "4",
+              "--niter_stat", "1", "--wd", str(wd)])
+    with h5.File(c.get_data_file_name()) as f:
+        assert f["iteration"][()] == 1
+    with h5.File(c.get_checkpoint_0_fname()) as f:
+        assert f["vorticity/complex"].keys() == ["0", "1"]
+
+
+def test_count_nonfinite_on_the_device():
+    from bfps_b200.solver import vorticity_equation
+    from bfps_b200 import ic
+    ve = vorticity_equation(16, precision="single")
+    w = ic.vorticity_ic(16, seed=3, dtype=np.complex64)
+    ve.set_cvorticity(w)
+    assert ve.count_nonfinite() == 0
+    w[1, 2, 3, 0] = np.nan
+    w[2, 1, 0, 2] = complex(0.0, np.inf)
+    ve.set_cvorticity(w)
+    assert ve.count_nonfinite() == 2
+    ve.close()
+
+
+def test_launcher_stops_on_nonfinite_state(tmp_path, golden):
+    """A NaN in the initial field (injected on the host) makes the run stop
+    with FloatingPointError before any statistics or checkpoint hold it."""
+    from bfps_b200.dns import DNS
+    src = tmp_path / "src"
+    src.mkdir()
+    w = np.array(golden["vorticity_0"])
+    w[1, 2, 3, 0] = np.nan
+    with h5.File(str(src / "B32p1e4_checkpoint_0.h5"), "w") as f:
+        f["vorticity/complex/0"] = w
+    c = DNS()
+    with pytest.raises(FloatingPointError):
+        c.launch(["NSVE", "-n", "32", "--src-simname", "B32p1e4", "--src-iteration", "0",
+                  "--simname", "nan", "--niter_todo", "4", "--niter_out", "4", "--niter_stat", "1",
+                  "--src-wd", str(src), "--wd", str(tmp_path / "run")])
+    with h5.File(c.get_data_file_name()) as f:
+        assert f["iteration"][()] == 0

@@ -58,3 +58,24 @@ def test_stats_anisotropic_box(dealias):
         assert np.abs(gm - wm).max() <= 1e-10 * np.abs(wm).max()
         assert np.abs(gh - wh).sum() <= 4 and gh.sum() == wh.sum()
     ve.close()
+
+
+def test_spectrum_bitwise_reproducible():
+    """The co-spectrum is summed in a fixed order: repeated calls, and a
+    second context holding the same field, give the same bits."""
+    from bfps_b200.solver import vorticity_equation
+    n = 64
+    w0 = ic.vorticity_ic(n, seed=21)
+    a = vorticity_equation(n, precision="double")
+    b = vorticity_equation(n, precision="double")
+    a.set_cvorticity(w0)
+    b.set_cvorticity(w0)
+    s1 = a.do_stats()
+    s2 = a.do_stats()
+    s3 = b.do_stats()
+    for key in ("velocity", "vorticity"):
+        assert np.array_equal(s1[key][0], s2[key][0])
+        assert np.array_equal(s1[key][0], s3[key][0])
+        assert np.array_equal(s1[key][1], s3[key][1])
+    a.close()
+    b.close()
