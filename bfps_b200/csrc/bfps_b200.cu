@@ -21,6 +21,7 @@
 #include "passes.cuh"
 #include "pressure.cuh"
 #include "stats.cuh"
+#include "xpass.cuh"
 
 using namespace bfg;
 
@@ -177,6 +178,20 @@ struct Prof {
 
 static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 
+// A kernel whose bounded wait on its own bulk copies ran out sets
+// g_bfg_wait_status (xpass.cuh); read (and cleared) after the work is done.
+static int check_wait_status(bfg_ctx* c) {
+    int st = 0;
+    CU(cudaMemcpyFromSymbol(&st, g_bfg_wait_status, sizeof(int)));
+    if (st) {
+        const int zero = 0;
+        CU(cudaMemcpyToSymbol(g_bfg_wait_status, &zero, sizeof(int)));
+        return fail(c, BFG_ECUDA, "a kernel's wait for its own bulk copies ran out");
+    }
+    return 0;
+}
+
+
 static KParams kparams(const bfg_ctx* c, double dt) {
     KParams k;
     k.nxv = c->nxv;
@@ -252,7 +267,22 @@ struct Engine {
     // one persistent launch of a row pass over nmem members
     template <int MODE, bool WRU>
     static int row(bfg_ctx* c, const Mem* mem, int nmem, Roles rl) {
-        if constexpr (MODE == RM_NONLIN && rnl_fused<N>()) {
+        if constexpr (MODE == RM_NONLIN && sizeof(T) == 4 && N == 512) {
+            // FP32 512^3: warp-per-row x pass (xpass.cuh)
+            constexpr size_t smem = xw_smem_bytes<N>();
+            auto kern = row_nonlin_warp<N, WRU>;
+            if (smem > (size_t)c->smem_optin)
+                return fail(c, BFG_EUNSUP, "x pass needs %zu bytes of shared memory", smem);
+            CU(ensure_smem(kern, smem, c->device));
+            const int rows_per = N * N;
+            const int nrows = rows_per * nmem;
+            const int grid = std::min(c->nsm, (nrows + xw::NWARP - 1) / xw::NWARP);
+            Prof pr(c, K_X);
+            kern<<<grid, xw::NWARP * 32, smem, c->stream>>>(
+                reinterpret_cast<const Member<float>*>(mem), rl,
+                reinterpret_cast<const cpx<float>*>(c->tw), rows_per, nrows);
+            return after_launch(c, "row_nonlin_warp");
+        } else if constexpr (MODE == RM_NONLIN && rnl_fused<T, N>()) {
             constexpr size_t smem = rnl_smem_bytes<T, N>();
             constexpr int ROWS = rnl_rows<T, N>();
             auto kern = row_nonlin<T, N, WRU>;
@@ -953,7 +983,7 @@ static int field_copy(bfg_ctx* c, int field_id, void* host, bool upload) {
         CU(cudaMemcpyAsync(host, c->wb, rows * hpitch, cudaMemcpyDeviceToHost, c->stream));
     }
     CU(cudaStreamSynchronize(c->stream));
-    return 0;
+    return check_wait_status(c);
 }
 
 int bfg_field_upload(bfg_ctx* c, int field_id, const void* host) {
@@ -1114,6 +1144,7 @@ int bfg_last_step_ms(bfg_ctx* c, double* ms) {
     if (!c || !ms) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
     CU(cudaEventSynchronize(c->ev1));
+    if (int rc = check_wait_status(c)) return rc;
     float f = 0;
     CU(cudaEventElapsedTime(&f, c->ev0, c->ev1));
     *ms = f;

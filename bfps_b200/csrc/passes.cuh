@@ -97,6 +97,15 @@ __host__ __device__ constexpr int pow2floor(int v) {
 }
 constexpr int SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per SM we plan for
 __host__ __device__ constexpr bool col_fz(int mode) { return mode >= 5 && mode <= 7; }
+// Radix cap per pass (FP32): the z passes (IZ, FZ) take 32-point butterflies
+// (two stages at 512^3 instead of three; measured 11 % faster for IZ), the
+// y passes keep radix 8, where the wider butterflies left threads idle
+// (fewer butterflies per stage than threads) and measured slower.
+template <typename T, int MODE>
+__host__ __device__ constexpr int col_mr() {
+    return col_max_radix<T, (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U ||
+                             (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN))>();
+}
 
 // tile row pitch (complex) for a tile of TKX kx columns: keeps every row
 // 16-byte aligned and breaks the worst bank patterns
@@ -256,7 +265,7 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     const double kz = kwrap<N>(l, kp.dkz);
     const double kx = fc.kx, ky = fc.ky;
     const double k2 = fc.kxy2 + kz * kz;
-    const int p = dif_position<N>(l);
+    const int p = dif_position<N, col_mr<T, MODE>()>(l);
     cpx<T> nl[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) nl[c] = tile[p * PR + col * 3 + c];
@@ -397,8 +406,9 @@ __device__ __forceinline__ void col_last_store(const cpx<T>* tile, int tid, cons
     constexpr int W = 3 * TKX;
     constexpr int PR = col_pitch<T, N, MODE>();
     constexpr bool INV = col_inverse(MODE);
-    constexpr int NST = plan_nstages(N);
-    constexpr int R = plan_radix(N, NST - 1);
+    constexpr int MR = col_mr<T, MODE>();
+    constexpr int NST = plan_nstages(N, MR);
+    constexpr int R = plan_radix(N, NST - 1, MR);
     constexpr int NW = PP * (N / R);
     constexpr size_t nxp3 = (size_t)(N / 2 + 4) * 3;
     const int nval = 3 * ncol;
@@ -413,7 +423,7 @@ __device__ __forceinline__ void col_last_store(const cpx<T>* tile, int tid, cons
         const int bufi = pp / W, q = pp % W;
         if (q >= nval) continue;
         cpx<T>* dst = mbuf(mb, (bufi == 0) ? rl.out0 : rl.out1) + (size_t)kx0 * 3 + q;
-        const int f0 = dif_frequency<N>(bb * R);
+        const int f0 = dif_frequency<N, MR>(bb * R);
 #pragma unroll
         for (int m = 0; m < R; ++m) dst[col_out_row<N, MODE>(a, f0 + (N / R) * m) * nxp3] = v[m];
     }
@@ -566,10 +576,11 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         // the tile holding only the Nyquist column transforms just its pencils
         using LYN = Lay<3, W, 1, PR>;
         constexpr int PN = NB * 3;
-        constexpr int NST = plan_nstages(N);
+        constexpr int MR = col_mr<T, MODE>();
+        constexpr int NST = plan_nstages(N, MR);
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
-            if (ncol == TKX) dif<T, N, INV, P, LY, 1, N>(tile, tw, tid, NT);
-            else dif<T, N, INV, PN, LYN, 1, N>(tile, tw, tid, NT);
+            if (ncol == TKX) dif<T, N, INV, P, LY, 1, N, MR>(tile, tw, tid, NT);
+            else dif<T, N, INV, PN, LYN, 1, N, MR>(tile, tw, tid, NT);
             __syncthreads();
             // ---- epilogue: one thread per mode (kz = l, kx = kx0 + col)
             const double ky = kwrap<N>(a, kp.dky);
@@ -597,10 +608,10 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             }
         } else {
             if (ncol == TKX) {
-                dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N>(tile, tw, tid, NT);
+                dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N, MR>(tile, tw, tid, NT);
                 col_last_store<T, N, MODE, P, false>(tile, tid, mb, rl, a, kx0, ncol);
             } else {
-                dif_range<T, N, 0, NST - 1, INV, PN, LYN, 1, N>(tile, tw, tid, NT);
+                dif_range<T, N, 0, NST - 1, INV, PN, LYN, 1, N, MR>(tile, tw, tid, NT);
                 col_last_store<T, N, MODE, PN, true>(tile, tid, mb, rl, a, kx0, ncol);
             }
         }
@@ -639,6 +650,16 @@ template <int N>
 __host__ __device__ constexpr int row_rl() { return (N / 2 + 4) * 3; }  // padded row, complex
 template <int N>
 __host__ __device__ constexpr int row_pl() { return N / 2 + 1; }  // odd pencil pitch
+// radix cap of the x transforms (length M = N/2): 8 (a cap of 16, two
+// stages at M = 256, left most threads of a tile idle in the mirror-paired
+// and last-stage phases and measured 30 % slower at 512^3)
+#ifndef BFG_ROW_MR_F32
+#define BFG_ROW_MR_F32 8
+#endif
+template <typename T, int M>
+__host__ __device__ constexpr int row_max_radix() {
+    return (sizeof(T) == 4 && M >= 64) ? BFG_ROW_MR_F32 : 8;
+}
 // shared memory for R rows: staging (two alternating buffers of interleaved
 // rows as they sit in HBM), pencils (one per component, odd pitch), output
 // rows (R2C only), twiddles and the digit-reversal table
@@ -773,7 +794,8 @@ row_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     const int tid = threadIdx.x;
 
     for (int i = tid; i < N; i += ROW_THREADS) tw[i] = tw_g[i];
-    for (int i = tid; i < M; i += ROW_THREADS) posn[i] = dif_position<M>(i);
+    constexpr int MRR = row_max_radix<T, M>();
+    for (int i = tid; i < M; i += ROW_THREADS) posn[i] = dif_position<M, MRR>(i);
     if constexpr (MODE == RM_R2C) {
         // padding columns of the output rows are written out: start them at 0
         for (int i = tid; i < ROWS * RL; i += ROW_THREADS) outr[i] = zero_c<T>();
@@ -825,7 +847,7 @@ row_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 c2r_pre<T, N>(st + (p / 3) * RL + (p % 3), S + p * PL, tw, k);
             }
             __syncthreads();
-            dif<T, M, true, NP, LP, 2, N>(S, tw, tid, ROW_THREADS);
+            dif<T, M, true, NP, LP, 2, N, MRR>(S, tw, tid, ROW_THREADS);
 
             if constexpr (MODE == RM_C2R || WRITE_RU) {
                 // real u (pencils of buffer 0) to rout in natural x order
@@ -868,7 +890,7 @@ row_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         }
         // forward: digit-reversed -> natural, then R2C post-processing into
         // interleaved rows (the staging rows of u, or the R2C output rows)
-        dit<T, M, false, 3 * ROWS, LP, 2, N>(S, tw, tid, ROW_THREADS);
+        dit<T, M, false, 3 * ROWS, LP, 2, N, MRR>(S, tw, tid, ROW_THREADS);
         cpx<T>* orow = (MODE == RM_R2C) ? outr : st;
         for (int e = tid; e < 3 * ROWS * (M / 2 + 1); e += ROW_THREADS) {
             const int k = e % (M / 2 + 1);
@@ -928,13 +950,14 @@ template <typename T, int N>
 __host__ __device__ constexpr int rnl_rg(int R) {
     return at_least_mod(rnl_w<T, N>(R) + 3 * rnl_pl<T, N>(R), nslot<T>(), nslot<T>() - 1);
 }
-template <int N>
+template <typename T, int N>
 __host__ __device__ constexpr int rnl_tw0() {
-    return (N / 2) / plan_radix(N / 2, 0) * (plan_radix(N / 2, 0) - 1);
+    return (N / 2) / plan_radix(N / 2, 0, row_max_radix<T, N / 2>()) *
+           (plan_radix(N / 2, 0, row_max_radix<T, N / 2>()) - 1);
 }
 template <typename T, int N>
 __host__ __device__ constexpr size_t rnl_bytes_for(int R) {
-    return (size_t)(2 * R * row_rl<N>() + R * rnl_rg<T, N>(R) + N + rnl_tw0<N>()) *
+    return (size_t)(2 * R * row_rl<N>() + R * rnl_rg<T, N>(R) + N + rnl_tw0<T, N>()) *
                sizeof(cpx<T>) +
            (size_t)(N / 2) * 4;
 }
@@ -969,8 +992,10 @@ template <typename T, int N>
 __host__ __device__ constexpr size_t rnl_smem_bytes() {
     return rnl_bytes_for<T, N>(rnl_rows<T, N>());
 }
-template <int N>
-__host__ __device__ constexpr bool rnl_fused() { return plan_nstages(N / 2) >= 2; }
+template <typename T, int N>
+__host__ __device__ constexpr bool rnl_fused() {
+    return plan_nstages(N / 2, row_max_radix<T, N / 2>()) >= 2;
+}
 
 // pencil p = c6 * ROWS + r: c6 < 3 the u pencils, c6 >= 3 the w pencils
 template <int ROWS, int RG, int PL, int W>
@@ -1031,11 +1056,12 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
            int tiles_per, int ntiles) {
     constexpr int RNL_THREADS = rnl_threads<T, N>();
     constexpr int M = N / 2;
-    constexpr int NS = plan_nstages(M);
-    constexpr int R0 = plan_radix(M, 0);
-    constexpr int S0 = M / R0;                 // span of stage 0
-    constexpr int H0 = S0 / 2;                 // mirror-paired units per pencil
-    constexpr int RZ = plan_radix(M, NS - 1);  // radix of the last stage (span 1)
+    constexpr int MRR = row_max_radix<T, M>();
+    constexpr int NS = plan_nstages(M, MRR);
+    constexpr int R0 = plan_radix(M, 0, MRR);
+    constexpr int S0 = M / R0;                      // span of stage 0
+    constexpr int H0 = S0 / 2;                      // mirror-paired units per pencil
+    constexpr int RZ = plan_radix(M, NS - 1, MRR);  // radix of the last stage (span 1)
     constexpr int NBZ = M / RZ;
     constexpr int ROWS = rnl_rows<T, N>();
     constexpr int RL = row_rl<N>();
@@ -1056,16 +1082,16 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
     cpx<T>* P = st + 2 * ROWS * RL;                     // ROWS regions of RG
     cpx<T>* tw = P + ROWS * RG;
     cpx<T>* tw0 = tw + N;  // stage-0 twiddles [j][q-1] = tw[2 j q]
-    int* posn = reinterpret_cast<int*>(tw0 + rnl_tw0<N>());
+    int* posn = reinterpret_cast<int*>(tw0 + rnl_tw0<T, N>());
     const int tid = threadIdx.x;
 
     for (int i = tid; i < N; i += RNL_THREADS) tw[i] = tw_g[i];
-    for (int i = tid; i < rnl_tw0<N>(); i += RNL_THREADS) {
+    for (int i = tid; i < rnl_tw0<T, N>(); i += RNL_THREADS) {
         const int j = i / (R0 - 1), q = i - j * (R0 - 1) + 1;
         tw0[i] = tw_g[2 * j * q];
     }
     if constexpr (WRITE_RU)
-        for (int i = tid; i < M; i += RNL_THREADS) posn[i] = dif_position<M>(i);
+        for (int i = tid; i < M; i += RNL_THREADS) posn[i] = dif_position<M, MRR>(i);
 
     auto issue = [&](int tt) {
         const int mm = tt / tiles_per, tl = tt - mm * tiles_per;
@@ -1153,9 +1179,9 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         cp_async_commit();
 
         // B: middle DIF stages over the six pencils of each row
-        dif_range<T, M, 1, NS - 1, true, 6 * ROWS, L6, 2, N>(P, tw, tid, RNL_THREADS);
+        dif_range<T, M, 1, NS - 1, true, 6 * ROWS, L6, 2, N, MRR>(P, tw, tid, RNL_THREADS);
         if constexpr (SPLIT) {
-            dif_stage<T, M, NS - 1, true, 3 * ROWS, LW, 2, N>(P, tw, tid, RNL_THREADS);
+            dif_stage<T, M, NS - 1, true, 3 * ROWS, LW, 2, N, MRR>(P, tw, tid, RNL_THREADS);
             __syncthreads();
         }
 
@@ -1267,7 +1293,7 @@ row_nonlin(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __re
         }
 
         // D: middle DIT stages over the w pencils
-        dit_range<T, M, NS - 2, 1, false, 3 * ROWS, LW, 2, N>(P, tw, tid, RNL_THREADS);
+        dit_range<T, M, NS - 2, 1, false, 3 * ROWS, LW, 2, N, MRR>(P, tw, tid, RNL_THREADS);
 
         // E: DIT stage 0 + R2C post-processing, w pencils -> output rows
         for (int e = tid; e < 3 * ROWS * H0; e += RNL_THREADS) {

@@ -1,0 +1,360 @@
+// Warp-per-row nonlinear x pass (the X pass of every RK stage), FP32, N = 512.
+//
+// Same result as row_nonlin (passes.cuh) -- per (z, y) row: C2R of the
+// velocity and vorticity rows (half-length complex transforms with the
+// C2R pre-processing), u x w / N^3 on the grid, R2C of the product -- but
+// organised around the warp instead of the CTA:
+//
+//   * each warp owns whole rows: one TMA bulk copy per input row brings the
+//     interleaved u and w rows (6240 bytes each) into the warp's own shared
+//     memory, completing on the warp's mbarrier;
+//   * a 256-point transform lives in registers, eight values per lane:
+//     one radix-8 butterfly over registers, then two exchanges through the
+//     warp's own shared buffer (radix-8 over 8-lane groups, radix-4 over
+//     4-lane groups), so no step of a row waits for another warp
+//     (__syncwarp only, no block barrier);
+//   * the product is formed in registers on the transformed values of all
+//     six transforms (every transform leaves the grid points in the same
+//     lane / register order);
+//   * the output row (and, in stage 1, the real velocity row u(t) for the
+//     tracers) leaves by TMA bulk stores.
+//
+// Lane layout of a 256-point transform (k frequency, n grid pair index,
+// z[n] = (x[2n], x[2n+1])): the spectrum side holds Z[l + 32 q] in lane l,
+// register q; the grid side holds z[n1 + 8 m1 + 64 m2] in lane 4 n1 + j,
+// register (m1 == j ? 0 : 4) + m2, m1 in {j, j + 4}.  With n = n1 + 8 n2,
+// k = l + 32 q: W_256^{nk} = W_256^{n1 l} W_8^{n1 q} W_32^{n2 l}, and the
+// 32-point factor splits again with n2 = m1 + 8 m2, l = l1 + 4 l2.
+//
+// Shared-memory pitches keep every exchange free of bank conflicts for
+// 8-byte accesses (half-warp wavefronts): [n1][l] rows of 36, [n1][l1][m1]
+// blocks of 68 / 17.
+#pragma once
+#include "passes.cuh"
+
+namespace bfg {
+
+// set by a kernel whose bounded wait on its own copies ran out (the host
+// reads it after a step and reports an error)
+__device__ int g_bfg_wait_status = 0;
+
+// ------------------------------------------------ TMA bulk copy helpers --
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// global -> shared bulk copy completing on bar (16-byte aligned, size a
+// multiple of 16); this GPU's own memory, no multicast
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for phase `parity` of bar; false (and the status word set)
+// if the copies have not landed after the limit
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (unsigned i = 0; i < (1u << 22); ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicExch(&g_bfg_wait_status, 1);
+    return false;
+}
+// shared -> global bulk store (bulk-group completion)
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// the sources of every committed bulk store have been read
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// every committed bulk store has completed
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+namespace xw {
+
+constexpr int NWARP = 12;              // warps per CTA, one CTA per SM
+constexpr int XP1 = 36;                // exchange [n1][l] row pitch
+constexpr int XP2 = 68, XQ2 = 17;      // exchange [n1][l1][m1] pitches
+constexpr int XBUF = 8 * XP2;          // 544 >= 8 * XP1, >= 256
+constexpr int T1P = 36;                // twiddle table [n1][l] row pitch
+
+template <int N>
+struct Smem {
+    static constexpr int RL = (N / 2 + 4) * 3;  // padded interleaved row (complex)
+    cpx<float> su[RL];                          // u row in, output row out
+    cpx<float> sw[RL];                          // w row in, real u row out
+    cpx<float> x[XBUF];                         // exchanges
+};
+
+// 256-point inverse transform (sign +): Z[l + 32 q] in v[q] -> grid order
+__device__ __forceinline__ void inv256(cpx<float> (&v)[8], cpx<float>* xb,
+                                       const cpx<float>* __restrict__ t1,
+                                       const cpx<float>* __restrict__ t2, int lane) {
+    dft<float, true, 8>(v);  // over q -> n1
+#pragma unroll
+    for (int n1 = 1; n1 < 8; ++n1) v[n1] = cmulc(v[n1], t1[n1 * T1P + lane]);  // W_256^{-n1 l}
+    __syncwarp();
+#pragma unroll
+    for (int n1 = 0; n1 < 8; ++n1) xb[n1 * XP1 + lane] = v[n1];
+    __syncwarp();
+    const int n1 = lane >> 2, l1 = lane & 3;
+#pragma unroll
+    for (int l2 = 0; l2 < 8; ++l2) v[l2] = xb[n1 * XP1 + l1 + 4 * l2];
+    dft<float, true, 8>(v);  // over l2 -> m1
+#pragma unroll
+    for (int m1 = 1; m1 < 8; ++m1) v[m1] = cmulc(v[m1], t2[l1 * 8 + m1]);  // W_32^{-l1 m1}
+    __syncwarp();
+#pragma unroll
+    for (int m1 = 0; m1 < 8; ++m1) xb[n1 * XP2 + l1 * XQ2 + m1] = v[m1];
+    __syncwarp();
+    const int j = lane & 3;
+    cpx<float> a[4], b[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        a[i] = xb[n1 * XP2 + i * XQ2 + j];
+        b[i] = xb[n1 * XP2 + i * XQ2 + j + 4];
+    }
+    dft<float, true, 4>(a);  // over l1 -> m2
+    dft<float, true, 4>(b);
+#pragma unroll
+    for (int m2 = 0; m2 < 4; ++m2) {
+        v[m2] = a[m2];
+        v[4 + m2] = b[m2];
+    }
+}
+
+// 256-point forward transform (sign -): grid order in -> Z[l + 32 q] in v[q]
+__device__ __forceinline__ void fwd256(cpx<float> (&v)[8], cpx<float>* xb,
+                                       const cpx<float>* __restrict__ t1,
+                                       const cpx<float>* __restrict__ t2, int lane) {
+    const int n1 = lane >> 2, j = lane & 3;
+    cpx<float> a[4], b[4];
+#pragma unroll
+    for (int m2 = 0; m2 < 4; ++m2) {
+        a[m2] = v[m2];
+        b[m2] = v[4 + m2];
+    }
+    dft<float, false, 4>(a);  // over m2 -> l1
+    dft<float, false, 4>(b);
+#pragma unroll
+    for (int l1 = 1; l1 < 4; ++l1) {
+        a[l1] = cmul(a[l1], t2[l1 * 8 + j]);      // W_32^{m1 l1}, m1 = j
+        b[l1] = cmul(b[l1], t2[l1 * 8 + j + 4]);  // m1 = j + 4
+    }
+    __syncwarp();
+#pragma unroll
+    for (int l1 = 0; l1 < 4; ++l1) {
+        xb[n1 * XP2 + l1 * XQ2 + j] = a[l1];
+        xb[n1 * XP2 + l1 * XQ2 + j + 4] = b[l1];
+    }
+    __syncwarp();
+    const int l1 = lane & 3;
+#pragma unroll
+    for (int m1 = 0; m1 < 8; ++m1) v[m1] = xb[n1 * XP2 + l1 * XQ2 + m1];
+    dft<float, false, 8>(v);  // over m1 -> l2
+#pragma unroll
+    for (int l2 = 0; l2 < 8; ++l2) v[l2] = cmul(v[l2], t1[n1 * T1P + l1 + 4 * l2]);  // W_256^{n1 l}
+    __syncwarp();
+#pragma unroll
+    for (int l2 = 0; l2 < 8; ++l2) xb[n1 * XP1 + l1 + 4 * l2] = v[l2];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = xb[i * XP1 + lane];
+    dft<float, false, 8>(v);  // over n1 -> q
+}
+
+}  // namespace xw
+
+// Launch: one CTA of NWARP warps per SM (persistent), 208 KB of shared
+// memory; warp w of CTA b takes rows b * NWARP + w, then strides by the
+// number of warps in the grid.  Rows run over all members of the launch.
+template <int N>
+__host__ __device__ constexpr size_t xw_smem_bytes() {
+    return (size_t)xw::NWARP * sizeof(xw::Smem<N>) +
+           (size_t)(N + 8 * xw::T1P + 32) * sizeof(cpx<float>) + xw::NWARP * 8;
+}
+
+template <int N, bool WRITE_RU>
+__global__ void __launch_bounds__(xw::NWARP * 32, 1)
+row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
+                const cpx<float>* __restrict__ tw_g, int rows_per, int nrows) {
+    static_assert(N == 512, "warp x pass: 256-point half-length transforms");
+    using namespace xw;
+    using C = cpx<float>;
+    constexpr int M = N / 2;
+    constexpr int RL = Smem<N>::RL;
+    constexpr unsigned ROW_BYTES = RL * sizeof(C);         // 6240
+    constexpr unsigned RU_BYTES = N * 3 * sizeof(float);   // 6144
+    static_assert(ROW_BYTES % 16 == 0 && RU_BYTES % 16 == 0, "bulk copy sizes");
+    static_assert(sizeof(Smem<N>) % 16 == 0, "warp regions stay 16-byte aligned");
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    Smem<N>* ws = reinterpret_cast<Smem<N>*>(smem_raw);
+    C* tw = reinterpret_cast<C*>(ws + NWARP);  // exp(-2 pi i m / N), m < N
+    C* t1 = tw + N;                            // [n1][l] = W_256^{n1 l}, pitch 36
+    C* t2 = t1 + 8 * T1P;                      // [l1][m1] = W_32^{l1 m1}
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(t2 + 32);
+
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int i = tid; i < N; i += blockDim.x) tw[i] = tw_g[i];
+    for (int i = tid; i < 8 * 32; i += blockDim.x) {
+        const int n1 = i >> 5, l = i & 31;
+        t1[n1 * T1P + l] = tw_g[(2 * n1 * l) % N];
+    }
+    if (tid < 32) t2[tid] = tw_g[16 * ((tid >> 3) * (tid & 7))];
+    if (tid < NWARP) mbar_init(&bars[tid], 1);
+    fence_mbar_init();
+    __syncthreads();
+
+    Smem<N>& S = ws[wid];
+    unsigned long long* bar = &bars[wid];
+    unsigned parity = 0;
+    const float inv_np = 1.0f / ((float)N * (float)N * (float)N);
+    const int gw = blockIdx.x * NWARP + wid, nw = gridDim.x * NWARP;
+
+    for (int row = gw; row < nrows; row += nw) {
+        const int m = row / rows_per;
+        const size_t r = (size_t)(row - m * rows_per);
+        const C* gu = mbuf(mem[m], rl.in0) + r * RL;
+        const C* gwv = mbuf(mem[m], rl.in1) + r * RL;
+        // the previous row's bulk stores must have read su / sw, and every
+        // lane's reads of them are ordered before the copies that refill them
+        bulk_wait_read();
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) {
+            mbar_expect_tx(bar, 2 * ROW_BYTES);
+            bulk_load(S.su, gu, ROW_BYTES, bar);
+            bulk_load(S.sw, gwv, ROW_BYTES, bar);
+        }
+        const bool ok = mbar_wait_bounded(bar, parity);
+        parity ^= 1u;
+        if (!ok) break;
+
+        // C2R pre-processing and inverse transforms: u -> U, w -> Wv
+        C U[3][8], Wv[3][8];
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            const C* st = f < 3 ? S.su : S.sw;
+            const int c = f % 3;
+            C v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = lane + 32 * q;
+                const C a = st[3 * k + c];
+                if (k == 0) {
+                    const float x0 = a.x, xm = st[3 * M + c].x;
+                    v[q] = mk<float>(x0 + xm, x0 - xm);
+                } else {
+                    v[q] = c2r_lo(a, st[3 * (M - k) + c], tw[k]);
+                }
+            }
+            xw::inv256(v, S.x, t1, t2, lane);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                if (f < 3) U[c][i] = v[i];
+                else Wv[c][i] = v[i];
+            }
+        }
+        // grid position of register i: n = n1 + 8 m1 + 64 m2
+        const int n1 = lane >> 2, j = lane & 3;
+        if constexpr (WRITE_RU) {
+            // u(t) in real space, [x][c] interleaved, through sw
+            float* rr = reinterpret_cast<float*>(S.sw);
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int n = n1 + 8 * (i < 4 ? j : j + 4) + 64 * (i & 3);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    rr[(2 * n) * 3 + c] = U[c][i].x;
+                    rr[(2 * n + 1) * 3 + c] = U[c][i].y;
+                }
+            }
+            fence_proxy_async();  // this lane's writes, visible to the bulk copy
+            __syncwarp();
+            if (lane == 0) {
+                bulk_store(mreal(mem[m], rl.rout) + r * (N * 3), rr, RU_BYTES);
+                bulk_commit();
+            }
+        }
+        // u x w / N^3 at every grid point (two per complex word)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            C p[3];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) {
+                const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+                const float tx = U[c1][i].x * Wv[c2][i].x - U[c2][i].x * Wv[c1][i].x;
+                const float ty = U[c1][i].y * Wv[c2][i].y - U[c2][i].y * Wv[c1][i].y;
+                p[cc] = mk<float>(tx * inv_np, ty * inv_np);
+            }
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) U[cc][i] = p[cc];
+        }
+        // forward transforms and R2C post-processing into su
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            C v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = U[c][i];
+            xw::fwd256(v, S.x, t1, t2, lane);
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 8; ++q) S.x[lane + 32 * q] = v[q];  // natural order
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = lane + 32 * q;
+                if (k == 0) {
+                    const C z0 = v[0];
+                    S.su[c] = mk<float>(z0.x + z0.y, 0.f);
+                    S.su[3 * M + c] = mk<float>(z0.x - z0.y, 0.f);
+                } else {
+                    S.su[3 * k + c] = r2c_lo(v[q], S.x[M - k], tw[k]);
+                }
+            }
+        }
+        // padding points of the output row carry zeros
+        if (lane < RL - 3 * (M + 1)) S.su[3 * (M + 1) + lane] = zero_c<float>();
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) {
+            bulk_store(mbuf(mem[m], rl.out0) + r * RL, S.su, ROW_BYTES);
+            bulk_commit();
+        }
+    }
+    bulk_wait_all();
+}
+
+}  // namespace bfg
