@@ -25,7 +25,8 @@
 
 using namespace bfg;
 
-#define BFG_VERSION "bfps_b200 0.1 (sm_100a)"
+#define BFG_VERSION "bfps_b200 0.2 (sm_100a)"
+
 
 struct bfg_ctx {
     int n = 0, nxv = 0, nxp = 0;

@@ -101,10 +101,13 @@ __host__ __device__ constexpr bool col_fz(int mode) { return mode >= 5 && mode <
 // (two stages at 512^3 instead of three; measured 11 % faster for IZ), the
 // y passes keep radix 8, where the wider butterflies left threads idle
 // (fewer butterflies per stage than threads) and measured slower.
+#ifndef BFG_FZ_WIDE
+#define BFG_FZ_WIDE 1
+#endif
 template <typename T, int MODE>
 __host__ __device__ constexpr int col_mr() {
     return col_max_radix<T, (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U ||
-                             (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN))>();
+                             (BFG_FZ_WIDE && MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN))>();
 }
 
 // tile row pitch (complex) for a tile of TKX kx columns: keeps every row

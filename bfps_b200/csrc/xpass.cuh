@@ -7,7 +7,10 @@
 //
 //   * each warp owns whole rows: one TMA bulk copy per input row brings the
 //     interleaved u and w rows (6240 bytes each) into the warp's own shared
-//     memory, completing on the warp's mbarrier;
+//     memory, completing on one of the warp's two mbarriers; the next row's
+//     u row is requested as soon as this row's u transforms are done, its w
+//     row as soon as this row's output has left, so both arrive while the
+//     warp still computes;
 //   * a 256-point transform lives in registers, eight values per lane:
 //     one radix-8 butterfly over registers, then two exchanges through the
 //     warp's own shared buffer (radix-8 over 8-lane groups, radix-4 over
@@ -111,8 +114,8 @@ constexpr int T1P = 36;                // twiddle table [n1][l] row pitch
 template <int N>
 struct Smem {
     static constexpr int RL = (N / 2 + 4) * 3;  // padded interleaved row (complex)
-    cpx<float> su[RL];                          // u row in, output row out
-    cpx<float> sw[RL];                          // w row in, real u row out
+    cpx<float> su[RL];                          // u row in, real u row out
+    cpx<float> sw[RL];                          // w row in, output row out
     cpx<float> x[XBUF];                         // exchanges
 };
 
@@ -201,7 +204,7 @@ __device__ __forceinline__ void fwd256(cpx<float> (&v)[8], cpx<float>* xb,
 template <int N>
 __host__ __device__ constexpr size_t xw_smem_bytes() {
     return (size_t)xw::NWARP * sizeof(xw::Smem<N>) +
-           (size_t)(N + 8 * xw::T1P + 32) * sizeof(cpx<float>) + xw::NWARP * 8;
+           (size_t)(N + 8 * xw::T1P + 32) * sizeof(cpx<float>) + xw::NWARP * 16;
 }
 
 template <int N, bool WRITE_RU>
@@ -232,39 +235,80 @@ row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
         t1[n1 * T1P + l] = tw_g[(2 * n1 * l) % N];
     }
     if (tid < 32) t2[tid] = tw_g[16 * ((tid >> 3) * (tid & 7))];
-    if (tid < NWARP) mbar_init(&bars[tid], 1);
+    if (tid < 2 * NWARP) mbar_init(&bars[tid], 1);
     fence_mbar_init();
     __syncthreads();
 
     Smem<N>& S = ws[wid];
-    unsigned long long* bar = &bars[wid];
-    unsigned parity = 0;
+    // bars[2 w]: the u row in su, bars[2 w + 1]: the w row in sw
+    unsigned long long* bar_u = &bars[2 * wid];
+    unsigned long long* bar_w = &bars[2 * wid + 1];
+    unsigned par_u = 0, par_w = 0;
     const float inv_np = 1.0f / ((float)N * (float)N * (float)N);
     const int gw = blockIdx.x * NWARP + wid, nw = gridDim.x * NWARP;
-
-    for (int row = gw; row < nrows; row += nw) {
+    auto row_src = [&](int row, int b) -> const C* {
         const int m = row / rows_per;
         const size_t r = (size_t)(row - m * rows_per);
-        const C* gu = mbuf(mem[m], rl.in0) + r * RL;
-        const C* gwv = mbuf(mem[m], rl.in1) + r * RL;
-        // the previous row's bulk stores must have read su / sw, and every
-        // lane's reads of them are ordered before the copies that refill them
+        return mbuf(mem[m], b ? rl.in1 : rl.in0) + r * RL;
+    };
+    // loads are issued by lane 0 after every lane's earlier reads of the
+    // destination (fence: ordered before the async proxy's writes) and after
+    // the bulk stores that read it (wait_group.read)
+    auto issue = [&](int row, int b) {
         bulk_wait_read();
         fence_proxy_async();
         __syncwarp();
         if (lane == 0) {
-            mbar_expect_tx(bar, 2 * ROW_BYTES);
-            bulk_load(S.su, gu, ROW_BYTES, bar);
-            bulk_load(S.sw, gwv, ROW_BYTES, bar);
+            unsigned long long* bb = b ? bar_w : bar_u;
+            mbar_expect_tx(bb, ROW_BYTES);
+            bulk_load(b ? S.sw : S.su, row_src(row, b), ROW_BYTES, bb);
         }
-        const bool ok = mbar_wait_bounded(bar, parity);
-        parity ^= 1u;
-        if (!ok) break;
+    };
+    if (gw < nrows) {
+        issue(gw, 0);
+        issue(gw, 1);
+    }
+    bool ok = true;
+    // grid position of register i of the grid side: n = n1 + 8 m1 + 64 m2
+    const int n1 = lane >> 2, j = lane & 3;
 
-        // C2R pre-processing and inverse transforms: u -> U, w -> Wv
+    for (int row = gw; row < nrows && ok; row += nw) {
+        const int m = row / rows_per;
+        const size_t r = (size_t)(row - m * rows_per);
+        const int next = row + nw;
         C U[3][8], Wv[3][8];
+        // u: C2R pre-processing and inverse transforms (su -> U)
+        ok = mbar_wait_bounded(bar_u, par_u);
+        par_u ^= 1u;
+        if (!ok) break;
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
+            if (f == 3) {
+                if constexpr (WRITE_RU) {
+                    // u(t) in real space, [x][c] interleaved, through su
+                    float* rr = reinterpret_cast<float*>(S.su);
+                    __syncwarp();
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int n = n1 + 8 * (i < 4 ? j : j + 4) + 64 * (i & 3);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            rr[(2 * n) * 3 + c] = U[c][i].x;
+                            rr[(2 * n + 1) * 3 + c] = U[c][i].y;
+                        }
+                    }
+                    fence_proxy_async();  // this lane's writes, visible to the bulk copy
+                    __syncwarp();
+                    if (lane == 0) {
+                        bulk_store(mreal(mem[m], rl.rout) + r * (N * 3), rr, RU_BYTES);
+                        bulk_commit();
+                    }
+                }
+                // w: wait for its row
+                ok = mbar_wait_bounded(bar_w, par_w);
+                par_w ^= 1u;
+                if (!ok) break;
+            }
             const C* st = f < 3 ? S.su : S.sw;
             const int c = f % 3;
             C v[8];
@@ -286,28 +330,9 @@ row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
                 else Wv[c][i] = v[i];
             }
         }
-        // grid position of register i: n = n1 + 8 m1 + 64 m2
-        const int n1 = lane >> 2, j = lane & 3;
-        if constexpr (WRITE_RU) {
-            // u(t) in real space, [x][c] interleaved, through sw
-            float* rr = reinterpret_cast<float*>(S.sw);
-            __syncwarp();
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int n = n1 + 8 * (i < 4 ? j : j + 4) + 64 * (i & 3);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    rr[(2 * n) * 3 + c] = U[c][i].x;
-                    rr[(2 * n + 1) * 3 + c] = U[c][i].y;
-                }
-            }
-            fence_proxy_async();  // this lane's writes, visible to the bulk copy
-            __syncwarp();
-            if (lane == 0) {
-                bulk_store(mreal(mem[m], rl.rout) + r * (N * 3), rr, RU_BYTES);
-                bulk_commit();
-            }
-        }
+        if (!ok) break;
+        // su is free: the next row's u streams in during the rest of this row
+        if (next < nrows) issue(next, 0);
         // u x w / N^3 at every grid point (two per complex word)
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -322,7 +347,8 @@ row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
 #pragma unroll
             for (int cc = 0; cc < 3; ++cc) U[cc][i] = p[cc];
         }
-        // forward transforms and R2C post-processing into su
+        // forward transforms and R2C post-processing into sw (free since the
+        // w transforms)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             C v[8];
@@ -338,21 +364,23 @@ row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
                 const int k = lane + 32 * q;
                 if (k == 0) {
                     const C z0 = v[0];
-                    S.su[c] = mk<float>(z0.x + z0.y, 0.f);
-                    S.su[3 * M + c] = mk<float>(z0.x - z0.y, 0.f);
+                    S.sw[c] = mk<float>(z0.x + z0.y, 0.f);
+                    S.sw[3 * M + c] = mk<float>(z0.x - z0.y, 0.f);
                 } else {
-                    S.su[3 * k + c] = r2c_lo(v[q], S.x[M - k], tw[k]);
+                    S.sw[3 * k + c] = r2c_lo(v[q], S.x[M - k], tw[k]);
                 }
             }
         }
         // padding points of the output row carry zeros
-        if (lane < RL - 3 * (M + 1)) S.su[3 * (M + 1) + lane] = zero_c<float>();
+        if (lane < RL - 3 * (M + 1)) S.sw[3 * (M + 1) + lane] = zero_c<float>();
         fence_proxy_async();
         __syncwarp();
         if (lane == 0) {
-            bulk_store(mbuf(mem[m], rl.out0) + r * RL, S.su, ROW_BYTES);
+            bulk_store(mbuf(mem[m], rl.out0) + r * RL, S.sw, ROW_BYTES);
             bulk_commit();
         }
+        // the next row's w once the store has read sw
+        if (next < nrows) issue(next, 1);
     }
     bulk_wait_all();
 }
