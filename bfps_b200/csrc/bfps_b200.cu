@@ -1095,6 +1095,16 @@ int bfg_lagrangian_acceleration(bfg_ctx* c, void* host) {
     return 0;
 }
 
+// host or device memory (unified addressing): cudaMemcpyDefault copies
+static bool is_host_memory(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged;
+}
+
 int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
     if (!c || !din || !dout) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
@@ -1104,12 +1114,17 @@ int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
     if ((rc = sync_member(c, c->fac_dt))) return rc;
     CU(cudaMemcpy2DAsync(c->wb, c->nxp * 3 * cb, din, c->nxv * 3 * cb, c->nxv * 3 * cb, N * N,
-                         cudaMemcpyDeviceToDevice, c->stream));
+                         cudaMemcpyDefault, c->stream));
     if ((rc = dispatch<OpIft>(c))) return rc;
-    CU(cudaMemset2DAsync(dout, (N + 2) * 3 * rb, 0, (N + 2) * 3 * rb, N * N, c->stream));
+    const bool host_out = is_host_memory(dout);
+    if (!host_out)
+        CU(cudaMemset2DAsync(dout, (N + 2) * 3 * rb, 0, (N + 2) * 3 * rb, N * N, c->stream));
     CU(cudaMemcpy2DAsync(dout, (N + 2) * 3 * rb, c->ru, N * 3 * rb, N * 3 * rb, N * N,
-                         cudaMemcpyDeviceToDevice, c->stream));
+                         cudaMemcpyDefault, c->stream));
     CU(cudaStreamSynchronize(c->stream));
+    if (host_out)  // padding points of every row
+        for (size_t r = 0; r < N * N; ++r)
+            std::memset(static_cast<char*>(dout) + (r * (N + 2) + N) * 3 * rb, 0, 2 * 3 * rb);
     return 0;
 }
 
@@ -1122,12 +1137,44 @@ int bfg_dft(bfg_ctx* c, const void* din, void* dout) {
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
     if ((rc = sync_member(c, c->fac_dt))) return rc;
     CU(cudaMemcpy2DAsync(c->ru, N * 3 * rb, din, (N + 2) * 3 * rb, N * 3 * rb, N * N,
-                         cudaMemcpyDeviceToDevice, c->stream));
+                         cudaMemcpyDefault, c->stream));
     if ((rc = dispatch<OpDft>(c))) return rc;
     CU(cudaMemcpy2DAsync(dout, c->nxv * 3 * cb, c->wb, c->nxp * 3 * cb, c->nxv * 3 * cb, N * N,
-                         cudaMemcpyDeviceToDevice, c->stream));
+                         cudaMemcpyDefault, c->stream));
     CU(cudaStreamSynchronize(c->stream));
     return 0;
+}
+
+int bfg_field_ift(bfg_ctx* c, int field_id) {
+    if (!c) return BFG_EINVAL;
+    if (field_id != BFG_FIELD_VELOCITY)
+        return fail(c, BFG_EINVAL, "bfg_field_ift: only the velocity field (%d)", BFG_FIELD_VELOCITY);
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    int rc = ensure_ru(c);
+    if (rc) return rc;
+    if ((rc = sync_member(c, c->fac_dt))) return rc;
+    // the transform reads wb and uses wa as scratch: the velocity moves to wb
+    CU(cudaMemcpyAsync(c->wb, c->wa, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+    if ((rc = dispatch<OpIft>(c))) return rc;
+    CU(cudaMemcpyAsync(c->wa, c->wb, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+int bfg_field_stats(bfg_ctx* c, const void* field, double max_estimate, int nbins, double* spec,
+                    double* mom, int64_t* hist) {
+    if (!c || !field || nbins < 1) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    int rc = sync_member(c, c->fac_dt);
+    if (rc) return rc;
+    // into v1 (free between steps), re-pitched to the device rows
+    const size_t N = c->n, cb = 2 * (size_t)c->real_bytes;
+    CU(cudaMemset2DAsync(c->v1, c->nxp * 3 * cb, 0, c->nxp * 3 * cb, N * N, c->stream));
+    CU(cudaMemcpy2DAsync(c->v1, c->nxp * 3 * cb, field, c->nxv * 3 * cb, c->nxv * 3 * cb, N * N,
+                         cudaMemcpyDefault, c->stream));
+    return dispatch<OpStats>(c, (int)B_V1, max_estimate, nbins, spec, mom, hist);
 }
 
 int bfg_get_iteration(const bfg_ctx* c, int* it) {

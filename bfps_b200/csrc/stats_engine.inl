@@ -31,7 +31,7 @@ int Engine<T, N>::stats(bfg_ctx* c, int cfield, double max_est, int nbins, doubl
     CU(cudaMemsetAsync(d_hist, 0, (size_t)nbins * 4 * 8, c->stream));
     const KParams kp = kparams(c, 0.0);
     Prof pr0(c, K_STATS);
-    const void* cptr = cfield == B_W0 ? c->w0 : c->wa;
+    const void* cptr = cfield == B_W0 ? c->w0 : (cfield == B_V1 ? c->v1 : c->wa);
     const size_t spec_smem = (size_t)spec_warps * spec_n * 8;
     CU(ensure_smem(spectrum_kernel<T, N>, spec_smem, c->device));
     spectrum_kernel<T, N><<<SPEC_BLOCKS, spec_warps * 32, spec_smem, c->stream>>>(

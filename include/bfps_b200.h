@@ -117,9 +117,25 @@ int bfg_lagrangian_acceleration(bfg_ctx* ctx, void* host);
 
 /* field::ift / field::dft (field.cpp:144-162) on a 3-vector field, using
  * caller device buffers in the reference layouts (complex: (n, n, n/2+1, 3),
- * real: (n, n, n+2, 3)); unnormalised like FFTW.  in may equal out. */
+ * real: (n, n, n+2, 3)); unnormalised like FFTW.  in may equal out; host
+ * or device memory (unified addressing). */
 int bfg_ift(bfg_ctx* ctx, const void* dev_complex_in, void* dev_real_out);
 int bfg_dft(bfg_ctx* ctx, const void* dev_real_in, void* dev_complex_out);
+
+/* field::ift of the context's velocity (cvelocity->ift(), as
+ * NSVEparticles::step calls it after compute_velocity, NSVEparticles.cpp:
+ * 35-36): the C2R of BFG_FIELD_VELOCITY into BFG_FIELD_RVELOCITY; the
+ * complex velocity is kept.  Other field ids: BFG_EINVAL. */
+int bfg_field_ift(bfg_ctx* ctx, int field_id);
+
+/* field::compute_stats (field.cpp:984-1040) of any complex 3-vector field
+ * in the reference layout (ny, nz, nx/2+1, 3), in host or device memory:
+ * co-spectrum (nshells, 3, 3), real-space moments (10, 4) and histograms
+ * (nbins, 4) with max_estimate per component (max_estimate sqrt(3) for the
+ * magnitude, field.cpp:1001-1004).  Uses the context's free RK buffer; the
+ * state and the velocity are untouched.  Outputs may be NULL. */
+int bfg_field_stats(bfg_ctx* ctx, const void* field, double max_estimate, int nbins,
+                    double* spec, double* mom, int64_t* hist);
 
 /* iteration counter (vorticity_equation::iteration). */
 int bfg_get_iteration(const bfg_ctx* ctx, int* iteration);

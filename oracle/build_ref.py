@@ -19,7 +19,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "libbfps_interp_ref.so")
-REF_CPP = "/root/reference/bfps/cpp"
+REF_ROOT = os.environ.get("BFPS_REFERENCE", "/root/reference")
+REF_CPP = os.path.join(REF_ROOT, "bfps", "cpp")
 
 
 def build(verbose=False):

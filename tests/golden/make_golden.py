@@ -20,7 +20,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 from bfps_b200 import h5  # noqa: E402
 
-SRC = "/root/reference/bfps/test/B32p1e4_checkpoint_0.h5"
+SRC = os.path.join(os.environ.get("BFPS_REFERENCE", "/root/reference"), "bfps", "test",
+                   "B32p1e4_checkpoint_0.h5")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "B32p1e4.npz")
 
 DATASETS = ["vorticity/complex/0", "vorticity/complex/32", "vorticity/complex/64",

@@ -20,7 +20,7 @@ import types
 
 import numpy as np
 
-TOOLS = "/root/reference/bfps/tools.py"
+TOOLS = os.path.join(os.environ.get("BFPS_REFERENCE", "/root/reference"), "bfps", "tools.py")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ic_vector_field_n16.npz")
 N = 16
 

@@ -152,6 +152,9 @@ class _FakeField:
     def get_cvorticity(self):
         return self.w.copy()
 
+    def count_nonfinite(self, field="vorticity"):
+        return int((~np.isfinite(self.w.real)).sum() + (~np.isfinite(self.w.imag)).sum())
+
     def step(self, dt, n=1):
         self.iteration += n
         self.w *= 1.0
@@ -232,6 +235,54 @@ def test_job_flow_with_a_stand_in_engine(tmp_path, golden, monkeypatch):
         assert sorted(int(k) for k in f["tracers0/velocity"].keys()) == list(range(1, 18))
         assert f["tracers0/velocity/5"][()].shape == (1, 50, 3)
         assert np.all(f["tracers0/acceleration/5"][()] == -5.0)
+
+
+def _stand_in(monkeypatch):
+    from bfps_b200 import solver
+    monkeypatch.setattr(solver, "vorticity_equation", _FakeField)
+    monkeypatch.setattr(solver, "particles_system", _FakeTracers)
+    monkeypatch.setattr(solver, "NSVEparticles_step", _fake_step)
+
+
+def test_stop_file_ends_main_loop(tmp_path, monkeypatch):
+    """code_base::check_stopping_condition (code_base.cpp:15-35): a file
+    stop_<simname> in the working directory, checked after every iteration
+    (direct_numerical_simulation.cpp:108-110), ends the job after the
+    current iteration with the final statistics and checkpoint; every
+    further job of the launch stops after one iteration too."""
+    _stand_in(monkeypatch)
+    wd = tmp_path / "run"
+    wd.mkdir()
+    (wd / "stop_st").write_text("")
+    c = dns.DNS()
+    c.launch(["NSVE", "-n", "16", "--simname", "st", "--niter_todo", "8", "--niter_out", "4",
+              "--niter_stat", "1", "--njobs", "2", "--wd", str(wd)])
+    with h5.File(c.get_data_file_name()) as f:
+        assert f["iteration"][()] == 2
+    with h5.File(c.get_checkpoint_0_fname()) as f:
+        assert f["vorticity/complex"].keys() == ["0", "1", "2"]
+
+
+def test_nonfinite_state_stops_the_run(tmp_path, golden, monkeypatch):
+    """A NaN in the state (here in the initial field) stops the run with
+    FloatingPointError before it reaches a statistics row or a checkpoint;
+    the host-side stand-in for the floating-point trapping the reference
+    enables (main_code.hpp:48-52)."""
+    _stand_in(monkeypatch)
+    src = tmp_path / "src"
+    src.mkdir()
+    w = np.array(golden["vorticity_0"])
+    w[1, 2, 3, 0] = np.nan
+    with h5.File(str(src / "B32p1e4_checkpoint_0.h5"), "w") as f:
+        f["vorticity/complex/0"] = w
+    c = dns.DNS()
+    with pytest.raises(FloatingPointError):
+        c.launch(["NSVE", "-n", "32", "--src-simname", "B32p1e4", "--src-iteration", "0",
+                  "--simname", "nan", "--niter_todo", "4", "--niter_out", "4", "--niter_stat", "1",
+                  "--src-wd", str(src), "--wd", str(tmp_path / "run")])
+    with h5.File(c.get_data_file_name()) as f:
+        assert f["iteration"][()] == 0
+        assert np.all(f["statistics/moments/velocity"][()] == 0)
 
 
 def test_command_line_and_postprocessing(tmp_path, golden, monkeypatch):

@@ -8,7 +8,8 @@ import pytest
 
 from bfps_b200 import h5
 
-FIXTURE = "/root/reference/bfps/test/B32p1e4_checkpoint_0.h5"
+FIXTURE = os.path.join(os.environ.get("BFPS_REFERENCE", "/root/reference"), "bfps", "test",
+                       "B32p1e4_checkpoint_0.h5")
 
 
 @pytest.mark.skipif(not os.path.exists(FIXTURE), reason="reference checkout absent")
