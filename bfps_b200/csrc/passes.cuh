@@ -535,6 +535,15 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             const double ky = kwrap<N>(a, kp.dky);
             // one point: kx, kx^2 + ky^2 and the storage-precision kx, ky of its
             // column given
+            // compute_velocity ends with field::symmetrize (field.cpp:903-978),
+            // which on the kx = 0 plane replaces every row ky = N - yy
+            // (0 < yy < N/2) by the conjugate of row yy, kz reversed.  The
+            // modes computed here already agree with that except on the kz =
+            // N/2 line, whose wavenumber +N/2 dkz does not change sign with
+            // ky (it matters where that line lies inside kM, e.g. for dk
+            // larger along y than along z): there u is taken from the mirror
+            // mode (N - ky, N/2), read from the source field.
+            const bool mirror_row = kx0 == 0 && a > N / 2;
             auto point = [&](int col, int l, double kxy2, T kxT, T kyT) {
                 const double kz = kwrap<N>(l, kp.dkz);
                 const double k2 = kxy2 + kz * kz;
@@ -543,9 +552,20 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 if (k2 <= kp.kM2 && k2 > 0.0) {
                     const T ik2 = (T)__drcp_rn(k2);
                     cpx<T> wv[3] = {w[0], w[1], w[2]};
-                    curl<T>(kxT, kyT, (T)kz, wv, u);
+                    const bool mirror = mirror_row && col == 0 && l == N / 2;
+                    if (mirror) {
+                        const cpx<T>* src = mbuf(mb, rl.in0) +
+                                            ((size_t)(N - a) * N + N / 2) * (N / 2 + 4) * 3;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) wv[c] = src[c];
+                    }
+                    curl<T>(kxT, mirror ? (T)kwrap<N>(N - a, kp.dky) : kyT, (T)kz, wv, u);
 #pragma unroll
                     for (int c = 0; c < 3; ++c) u[c] = scale(u[c], ik2);
+                    if (mirror) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) u[c] = conjg(u[c]);
+                    }
                 } else {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) u[c] = zero_c<T>();

@@ -169,7 +169,10 @@ def test_fp64_smooth_filter_shared_keys():
     """dky = 1.3: distinct k^2 share a filter key round(k^2 / dk^2), and the
     reference keeps the value written last in CLOOP order
     (kspace.cpp:119-150, applied by kspace.cpp:479); the engine's table and
-    the oracle's keyed table give the same step."""
+    the oracle's keyed table give the same step.  With kM set by the y axis
+    the kz = N/2 line lies inside kM, where compute_velocity's symmetrize
+    (field.cpp:903-978) takes the kx = 0 velocity of rows ky > N/2 from
+    their mirror rows."""
     from bfps_b200.solver import vorticity_equation
     n, dk = 32, (1.0, 1.3, 1.0)
     ve = vorticity_equation(n, n, n, *dk, precision="double")
