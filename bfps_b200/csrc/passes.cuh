@@ -97,17 +97,22 @@ __host__ __device__ constexpr int pow2floor(int v) {
 }
 constexpr int SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per SM we plan for
 __host__ __device__ constexpr bool col_fz(int mode) { return mode >= 5 && mode <= 7; }
-// Radix cap per pass (FP32): the z passes (IZ, FZ) take 32-point butterflies
-// (two stages at 512^3 instead of three; measured 11 % faster for IZ), the
-// y passes keep radix 8, where the wider butterflies left threads idle
-// (fewer butterflies per stage than threads) and measured slower.
+// Radix cap per pass (FP32): 32-point butterflies (two stages at 512^3
+// instead of three) in every column pass; with the two-CTA launch shape
+// below they measured faster for all of them (IZ 1.49 -> 1.33, IY 1.79 ->
+// 1.60, FY 0.88 -> 0.75 ms at 512^3).  A cap of 16 measured slower
+// everywhere.
 #ifndef BFG_FZ_WIDE
 #define BFG_FZ_WIDE 1
+#endif
+#ifndef BFG_Y_WIDE
+#define BFG_Y_WIDE 1
 #endif
 template <typename T, int MODE>
 __host__ __device__ constexpr int col_mr() {
     return col_max_radix<T, (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U ||
-                             (BFG_FZ_WIDE && MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN))>();
+                             (BFG_FZ_WIDE && MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN) ||
+                             (BFG_Y_WIDE && (MODE == CM_Y_INV2 || MODE == CM_Y_FWD1)))>();
 }
 
 // tile row pitch (complex) for a tile of TKX kx columns: keeps every row
@@ -124,12 +129,12 @@ __host__ __device__ constexpr int col_pitch_for(int tkx) {
 __host__ __device__ constexpr int col_nrk(int mode) {
     return mode == CM_FZ_RK1 ? 1 : ((mode == CM_FZ_RK2 || mode == CM_FZ_RK3) ? 2 : 0);
 }
-// Launch shape of a column pass.  The IZ passes (which read half of what
-// they write) run two 256-thread CTAs per SM with one tile buffer each, where
-// such a tile still has rows of at least 96 bytes: one CTA's barrier waits
-// and loads are covered by the other CTA's work (measured faster for IZ,
-// slower for IY and FY).  Otherwise one 512-thread CTA per SM with two tile
-// buffers, the next tile loading while this one is transformed.
+// Launch shape of a column pass.  Two 256-thread CTAs per SM with one tile
+// buffer each, where such a tile still has rows of at least 96 bytes: one
+// CTA's barrier waits, loads and (FZ) epilogue are covered by the other
+// CTA's work.  Otherwise one 512-thread CTA per SM with two tile buffers,
+// the next tile loading while this one is transformed.  Three CTAs per SM
+// for the one-buffer passes measured slower (FY 0.75 -> 1.03 ms).
 // shared memory: nbuf tile buffers + twiddles
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t col_bytes_nb(int tkx, int nbuf) {
@@ -150,20 +155,37 @@ __host__ __device__ constexpr int col_tkx_sel(int nbuf, size_t budget) {
                ? N / 2 + 1
                : col_tkx_fit<T, N, MODE>(16, nbuf, budget);
 }
+// Measured at 512^3 FP32: FZ 2.06 -> 1.86 ms, IY 1.79 -> 1.60 ms (with the
+// radix cap of 32), against one 512-thread CTA with two buffers.
+#ifndef BFG_FZ_TWO
+#define BFG_FZ_TWO 1
+#endif
+#ifndef BFG_Y_TWO
+#define BFG_Y_TWO 1
+#endif
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr bool col_two() {
-    return (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) &&
+    return (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U ||
+            (BFG_FZ_TWO && MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) ||
+            (BFG_Y_TWO && (MODE == CM_Y_INV2 || MODE == CM_Y_FWD1))) &&
            col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / 2) * 3 * (int)sizeof(cpx<T>) >= 96;
 }
+// CTAs per SM of the single-buffer launch shape for the passes with one
+// buffer per tile (FY, FZ)
+#ifndef BFG_NB1_CTAS
+#define BFG_NB1_CTAS 2
+#endif
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_threads() { return col_two<T, N, MODE>() ? 256 : 512; }
 template <typename T, int N, int MODE>
-__host__ __device__ constexpr int col_ctas() { return col_two<T, N, MODE>() ? 2 : 1; }
+__host__ __device__ constexpr int col_ctas() {
+    return col_two<T, N, MODE>() ? (col_nb(MODE) == 1 ? BFG_NB1_CTAS : 2) : 1;
+}
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_nbuf() { return col_two<T, N, MODE>() ? 1 : 2; }
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr int col_tkx() {
-    return col_two<T, N, MODE>() ? col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / 2)
+    return col_two<T, N, MODE>() ? col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / col_ctas<T, N, MODE>())
                                  : col_tkx_sel<T, N, MODE>(2, SMEM_BUDGET);
 }
 template <typename T, int N, int MODE>
@@ -200,6 +222,15 @@ __device__ __forceinline__ void divfree(A kx, A ky, A kz, A inv_k2, cpx<A>* a) {
 
 template <typename T>
 __device__ __forceinline__ cpx<T> zero_c() { return mk<T>((T)0, (T)0); }
+
+// 1 / k^2 in the storage precision: correctly rounded in FP64; in FP32 the
+// reciprocal of k^2 rounded to FP32 (within an FP32 ulp of the FP64 value
+// rounded, without the FP64 reciprocal sequence)
+template <typename T>
+__device__ __forceinline__ T inv_k2(double k2) {
+    if constexpr (sizeof(T) == 4) return __frcp_rn(__double2float_rn(k2));
+    else return (T)__drcp_rn(k2);
+}
 
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
@@ -305,7 +336,8 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     }
     // force_divfree on the nonlinear term; zero mode cleared
     const bool kzero = (a == 0 && l == 0 && ix == 0);
-    if (k2 > 0.0) divfree<T>(fc.kxT, fc.kyT, kzT, (T)__drcp_rn(k2), tt);
+    const T ik2 = inv_k2<T>(k2);
+    if (k2 > 0.0) divfree<T>(fc.kxT, fc.kyT, kzT, ik2, tt);
     if (kzero) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) tt[c] = zero_c<T>();
@@ -338,7 +370,7 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
                                   (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 * third)
                           : v0[c];
         // final force_divfree of the state (vorticity_equation.cpp:436)
-        if (k2 > 0.0) divfree<T>(fc.kxT, fc.kyT, kzT, (T)__drcp_rn(k2), o);
+        if (k2 > 0.0) divfree<T>(fc.kxT, fc.kyT, kzT, ik2, o);
         if (kzero) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
@@ -550,7 +582,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 cpx<T>* w = &tile[l * PR + WSRC + col * 3];
                 cpx<T> u[3];
                 if (k2 <= kp.kM2 && k2 > 0.0) {
-                    const T ik2 = (T)__drcp_rn(k2);
+                    const T ik2 = inv_k2<T>(k2);
                     cpx<T> wv[3] = {w[0], w[1], w[2]};
                     const bool mirror = mirror_row && col == 0 && l == N / 2;
                     if (mirror) {
