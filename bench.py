@@ -284,6 +284,8 @@ def run_ours(args, cfg):
     dev = local
     w0, pos = make_inputs(cfg, seed=rank)
     ve, ps = build_solver(cfg, w0, pos, dev)
+    # the column passes' schedules for this grid and precision (bfg_autotune)
+    tuned = ve.autotune(reps=3) if not args.no_tune else ve.schedules()
     L = _lib.lib()
     dt = cfg["dt"]
     # warm-up
@@ -400,6 +402,8 @@ def run_ours(args, cfg):
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "schedules": {k: {"schedule": v[0], "ms": [round(v[1], 4), round(v[2], 4)]}
+                      for k, v in tuned.items()},
     }
     if ps.n > 0 and world == 1:
         out["acceleration_sampling"] = acceleration_report(ve, ps, cfg)
@@ -466,6 +470,15 @@ def run_ensemble(args, cfg):
     ens = ensemble(local)
     for (fs, ps), r in zip(members, reqs):
         ens.add(fs, r.dt, ps)
+    # schedules of the column passes, timed on each size group as the
+    # ensemble launches it (all members of a size in one launch)
+    if args.no_tune:
+        tuned = {}
+        for fs, _ in members:
+            k = sum(1 for g, _ in members if g.nx == fs.nx)
+            tuned.setdefault(fs.nx, fs.schedules(members=k))
+    else:
+        tuned = ens.autotune(reps=3)
     ens.step(args.warmup)
     ens.last_ms()
     clocks = ClockSampler(local)
@@ -539,6 +552,8 @@ def run_ensemble(args, cfg):
                 "d2h_bytes_per_step": int(nbytes), "steps": e2e_steps},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "schedules": {str(n): {k: {"schedule": v[0], "ms": [round(v[1], 4), round(v[2], 4)]}
+                               for k, v in t.items()} for n, t in tuned.items()},
     }
     ens.close()
     for fs, ps in members:
@@ -796,6 +811,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=90.0,
                     help="seconds of whole CPU steps the reference arm times (at least 3 steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default column-pass schedules (no bfg_autotune)")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the FP32-vs-FP64 error report of the FP32 workloads")
     ap.add_argument("--grid", type=int, default=None,

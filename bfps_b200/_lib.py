@@ -69,6 +69,10 @@ SIGNATURES = {
     "bfg_rspace_stats_noalloc": (_i, [_vp, _i, _i, _i, _i, _d, _i, _vp, _vp, _vp]),
     "bfg_check_finite": (_i, [_vp, _i, _c.POINTER(_i64)]),
     "bfg_field_ift": (_i, [_vp, _i]),
+    "bfg_autotune": (_i, [_vp, _i]),
+    "bfg_ens_autotune": (_i, [_vp, _i]),
+    "bfg_tune_get": (_i, [_vp, _i, _i, _c.POINTER(_i), _pd, _pd]),
+    "bfg_tune_set": (_i, [_vp, _i, _i, _i]),
     "bfg_field_stats": (_i, [_vp, _vp, _d, _i, _pd, _pd, _pi64]),
     "bfg_ens_create": (_i, [_c.POINTER(_vp), _i]),
     "bfg_ens_destroy": (None, [_vp]),

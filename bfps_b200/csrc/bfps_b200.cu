@@ -9,9 +9,12 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -233,36 +236,173 @@ static cudaError_t ensure_smem(K kernel, size_t bytes, int device) {
 
 static double kwrap_h(int i, int N, double dk) { return dk * (double)(i <= N / 2 ? i : i - N); }
 
+// --------------------------------------------------------- autotuning --
+// Column-pass schedule (passes.cuh: 0 or 1) per (device, grid size, real
+// bytes, pass kind, members per launch).  The member count is part of the key
+// because the better schedule depends on how many tiles one launch holds: a
+// lone 64^3 context and a group of sixteen 64^3 ensemble members choose
+// differently.  Filled by bfg_autotune (one member), bfg_ens_autotune (each
+// size group of an ensemble), bfg_tune_set and, where the environment
+// variable BFPS_B200_TUNE_CACHE names a file, by the choices recorded there
+// by earlier runs on a device of the same name (one line per choice: device
+// name, N, real bytes, pass kind, members, schedule, and the two measured
+// times in ms).  Entries not tuned for that exact key use schedule 0.
+struct TuneEntry {
+    int sched = 0;
+    double ms0 = 0, ms1 = 0;
+};
+static std::mutex g_tune_mu;
+using TuneKey = std::tuple<int, int, int, int, int>;  // device, N, real bytes, kind, members
+static std::map<TuneKey, TuneEntry> g_tune;
+static std::map<int, bool> g_tune_loaded;  // device -> cache file read
+
+static int col_kind(int mode) {
+    return (mode == CM_IZ_VEL || mode == CM_IZ_PLAIN || mode == CM_IZ_U) ? K_IZ
+           : (mode == CM_Y_INV1 || mode == CM_Y_INV2)                  ? K_IY
+           : (mode == CM_Y_FWD1)                                      ? K_FY
+                                                                      : K_FZ;
+}
+static std::string device_name(int dev) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return "unknown";
+    }
+    std::string n = p.name;
+    for (char& ch : n)
+        if (ch == ' ') ch = '_';
+    return n;
+}
+// read the cache file's entries for this device (g_tune_mu held)
+static void tune_load_locked(int dev) {
+    if (g_tune_loaded[dev]) return;
+    g_tune_loaded[dev] = true;
+    const char* path = std::getenv("BFPS_B200_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    const std::string me = device_name(dev);
+    char name[256];
+    int n, rb, kind, nmem, sched;
+    double ms0, ms1;
+    while (std::fscanf(f, "%255s %d %d %d %d %d %lf %lf", name, &n, &rb, &kind, &nmem, &sched, &ms0,
+                       &ms1) == 8)
+        if (me == name && (sched == 0 || sched == 1) && nmem >= 1) {
+            TuneEntry& e = g_tune[TuneKey(dev, n, rb, kind, nmem)];
+            e.sched = sched;
+            e.ms0 = ms0;
+            e.ms1 = ms1;
+        }
+    std::fclose(f);
+}
+static int tuned_schedule(int dev, int n, int rb, int kind, int nmem) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked(dev);
+    auto it = g_tune.find(TuneKey(dev, n, rb, kind, nmem));
+    return it == g_tune.end() ? 0 : it->second.sched;
+}
+// Schedule 1 replaces the default only when it is faster by more than this
+// fraction: the tuner times one launch at a time, and schedule 0 (two CTAs
+// per SM) shares the SMs better with the concurrent launches of an
+// ensemble's other size groups, so near-ties go to it.
+constexpr double TUNE_MARGIN = 0.02;
+
+// record measured times (ms[kind * 2 + schedule]) for nmem members per
+// launch, the chosen schedule, and append them to the cache file
+static void tune_store(int dev, int n, int rb, int nmem, const double* ms) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked(dev);
+    const char* path = std::getenv("BFPS_B200_TUNE_CACHE");
+    FILE* f = (path && *path) ? std::fopen(path, "a") : nullptr;
+    const std::string name = device_name(dev);
+    for (int kind : {(int)K_IZ, (int)K_IY, (int)K_FY, (int)K_FZ}) {
+        TuneEntry e;
+        e.ms0 = ms[2 * kind];
+        e.ms1 = ms[2 * kind + 1];
+        e.sched = e.ms1 < e.ms0 * (1.0 - TUNE_MARGIN) ? 1 : 0;
+        g_tune[TuneKey(dev, n, rb, kind, nmem)] = e;
+        if (f)
+            std::fprintf(f, "%s %d %d %d %d %d %.6f %.6f\n", name.c_str(), n, rb, kind, nmem, e.sched,
+                         e.ms0, e.ms1);
+    }
+    if (f) std::fclose(f);
+}
+
 // ------------------------------------------------------------- engine --
 template <typename T, int N>
 struct Engine {
     using C = cpx<T>;
     using Mem = Member<T>;
 
-    // one persistent launch of a column pass over nmem members
+    // one persistent launch of a column pass over nmem members, in the
+    // schedule the autotuner chose for this grid, precision, pass and
+    // member count
     template <int MODE>
     static int col(bfg_ctx* c, const Mem* mem, int nmem, Roles rl) {
-        constexpr int TKX = col_tkx<T, N, MODE>();
-        constexpr size_t smem = col_smem_bytes<T, N, MODE>();
-        auto kern = col_pass<T, N, MODE>;
+        return tuned_schedule(c->device, N, (int)sizeof(T), col_kind(MODE), nmem) == 1
+                   ? col_s<MODE, 1>(c, mem, nmem, rl)
+                   : col_s<MODE, 0>(c, mem, nmem, rl);
+    }
+    template <int MODE, int S>
+    static int col_s(bfg_ctx* c, const Mem* mem, int nmem, Roles rl) {
+        constexpr int TKX = col_tkx<T, N, MODE, S>();
+        constexpr size_t smem = col_smem_bytes<T, N, MODE, S>();
+        auto kern = col_pass<T, N, MODE, S>;
         if (smem > (size_t)c->smem_optin)
             return fail(c, BFG_EUNSUP, "column pass needs %zu bytes of shared memory", smem);
         CU(ensure_smem(kern, smem, c->device));
         const int ntx = (N / 2 + 1 + TKX - 1) / TKX;
         const int tiles_per = ntx * N;
         const int ntiles = tiles_per * nmem;
-        const int grid = std::min(ntiles, c->nsm * col_ctas<T, N, MODE>());
-        constexpr int kind = (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U) ? K_IZ
-                             : (MODE == CM_Y_INV1 || MODE == CM_Y_INV2)                  ? K_IY
-                             : (MODE == CM_Y_FWD1)                                      ? K_FY
-                                                                                        : K_FZ;
-        Prof pr(c, kind);
+        const int grid = std::min(ntiles, c->nsm * col_ctas<T, N, MODE, S>());
+        Prof pr(c, col_kind(MODE));
         // dynamic tile order for the IZ passes with at least 8 tiles per CTA
         constexpr bool iz = MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U;
         int* tctr = (iz && ntiles >= 8 * grid) ? c->tctr : nullptr;
-        kern<<<grid, col_threads<T, N, MODE>(), smem, c->stream>>>(mem, rl, (const C*)c->tw, ntx, tiles_per,
-                                                     ntiles, tctr);
+        kern<<<grid, col_threads<T, N, MODE, S>(), smem, c->stream>>>(mem, rl, (const C*)c->tw, ntx,
+                                                                     tiles_per, ntiles, tctr);
         return after_launch(c, "col_pass");
+    }
+
+    // bfg_autotune / bfg_ens_autotune: both schedules of each column pass
+    // over the nmem members at m (roles that write only the work buffers
+    // wa, wb); ms[kind * 2 + schedule] receives the mean launch time
+    static int tune(bfg_ctx* c, const Mem* m, int nmem, int reps, double* ms) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+            if (e0) cudaEventDestroy(e0);
+            cudaGetLastError();
+            return fail(c, BFG_ECUDA, "cannot create timing events");
+        }
+        struct Ev {
+            cudaEvent_t a, b;
+            ~Ev() { cudaEventDestroy(a), cudaEventDestroy(b); }
+        } ev{e0, e1};
+        auto time_it = [&](auto launch, double* out) -> int {
+            int rc = launch();  // warm-up
+            if (rc) return rc;
+            CU(cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < reps; ++r)
+                if ((rc = launch())) return rc;
+            CU(cudaEventRecord(e1, c->stream));
+            CU(cudaEventSynchronize(e1));
+            float f = 0.f;
+            CU(cudaEventElapsedTime(&f, e0, e1));
+            *out = f / reps;
+            return 0;
+        };
+        const Roles r_iz = roles(B_W0, B_NONE, B_WA, B_WB), r_iy = roles(B_WA, B_WB, B_WA, B_WB),
+                    r_fy = roles(B_WA, B_NONE, B_WA, B_NONE),
+                    r_fz = roles(B_WA, B_NONE, B_WB, B_NONE, B_W0, B_V1, B_W0);
+        int rc;
+        if ((rc = time_it([&] { return col_s<CM_IZ_VEL, 0>(c, m, nmem, r_iz); }, &ms[2 * K_IZ]))) return rc;
+        if ((rc = time_it([&] { return col_s<CM_IZ_VEL, 1>(c, m, nmem, r_iz); }, &ms[2 * K_IZ + 1]))) return rc;
+        if ((rc = time_it([&] { return col_s<CM_Y_INV2, 0>(c, m, nmem, r_iy); }, &ms[2 * K_IY]))) return rc;
+        if ((rc = time_it([&] { return col_s<CM_Y_INV2, 1>(c, m, nmem, r_iy); }, &ms[2 * K_IY + 1]))) return rc;
+        if ((rc = time_it([&] { return col_s<CM_Y_FWD1, 0>(c, m, nmem, r_fy); }, &ms[2 * K_FY]))) return rc;
+        if ((rc = time_it([&] { return col_s<CM_Y_FWD1, 1>(c, m, nmem, r_fy); }, &ms[2 * K_FY + 1]))) return rc;
+        if ((rc = time_it([&] { return col_s<CM_FZ_RK2, 0>(c, m, nmem, r_fz); }, &ms[2 * K_FZ]))) return rc;
+        return time_it([&] { return col_s<CM_FZ_RK2, 1>(c, m, nmem, r_fz); }, &ms[2 * K_FZ + 1]);
     }
 
     // one persistent launch of a row pass over nmem members
@@ -516,6 +656,12 @@ struct OpIft {
 template <typename T, int N>
 struct OpDft {
     static int run(bfg_ctx* c) { return Engine<T, N>::dft_ru(c); }
+};
+template <typename T, int N>
+struct OpTune {
+    static int run(bfg_ctx* c, int reps, double* ms) {
+        return Engine<T, N>::tune(c, Engine<T, N>::self(c), 1, reps, ms);
+    }
 };
 template <typename T, int N>
 struct OpStats {
@@ -1277,6 +1423,46 @@ int bfg_check_finite(bfg_ctx* c, int field_id, int64_t* nonfinite) {
     return 0;
 }
 
+static bool col_kind_valid(int kind) {
+    return kind == K_IZ || kind == K_IY || kind == K_FY || kind == K_FZ;
+}
+
+int bfg_autotune(bfg_ctx* c, int reps) {
+    if (!c) return BFG_EINVAL;
+    if (reps < 1) reps = 1;
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    const double dt = std::isnan(c->fac_dt) ? 1e-3 : c->fac_dt;
+    int rc = ensure_factors(c, dt);
+    if (rc) return rc;
+    if ((rc = sync_member(c, dt))) return rc;
+    double ms[2 * BFG_NKINDS] = {0};
+    if ((rc = dispatch<OpTune>(c, reps, ms))) return rc;
+    tune_store(c->device, c->n, c->real_bytes, 1, ms);
+    return 0;
+}
+
+int bfg_tune_get(const bfg_ctx* c, int kind, int members, int* schedule, double* ms0, double* ms1) {
+    if (!c || !col_kind_valid(kind) || members < 1) return BFG_EINVAL;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked(c->device);
+    auto it = g_tune.find(TuneKey(c->device, c->n, c->real_bytes, kind, members));
+    const TuneEntry e = it == g_tune.end() ? TuneEntry() : it->second;
+    if (schedule) *schedule = e.sched;
+    if (ms0) *ms0 = e.ms0;
+    if (ms1) *ms1 = e.ms1;
+    return 0;
+}
+
+int bfg_tune_set(bfg_ctx* c, int kind, int members, int schedule) {
+    if (!c || !col_kind_valid(kind) || members < 1 || (schedule != 0 && schedule != 1))
+        return BFG_EINVAL;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked(c->device);
+    g_tune[TuneKey(c->device, c->n, c->real_bytes, kind, members)].sched = schedule;
+    return 0;
+}
+
 // ------------------------------------------------------------ tracers --
 // scatter device-order arrays (width doubles per tracer) into creation order
 __global__ void to_creation_order(const double* __restrict__ src, const int64_t* __restrict__ corder,
@@ -1842,6 +2028,24 @@ static int ens_stage(bfg_ens* e, EnsGroup* g, int s) {
     return e->real_bytes == 4 ? ens_group_stage<float>(g, s) : ens_group_stage<double>(g, s);
 }
 
+// both column-pass schedules timed on a whole size group (one launch over
+// all its members, as bfg_ens_step issues them)
+template <typename T>
+static int ens_group_tune(EnsGroup* g, int reps, double* ms) {
+    const Member<T>* mem = (const Member<T>*)g->dmem;
+    const int nm = (int)g->members.size();
+    switch (g->n) {
+        case 16: return Engine<T, 16>::tune(&g->launcher, mem, nm, reps, ms);
+        case 32: return Engine<T, 32>::tune(&g->launcher, mem, nm, reps, ms);
+        case 64: return Engine<T, 64>::tune(&g->launcher, mem, nm, reps, ms);
+        case 128: return Engine<T, 128>::tune(&g->launcher, mem, nm, reps, ms);
+        case 256: return Engine<T, 256>::tune(&g->launcher, mem, nm, reps, ms);
+        case 512: return Engine<T, 512>::tune(&g->launcher, mem, nm, reps, ms);
+        case 1024: return Engine<T, 1024>::tune(&g->launcher, mem, nm, reps, ms);
+    }
+    return BFG_EUNSUP;
+}
+
 // (re)build groups, member arrays and graphs after membership changes
 static int ens_prepare(bfg_ens* e) {
     if (!e->dirty) return 0;
@@ -2111,6 +2315,27 @@ int bfg_ens_step(bfg_ens* e, int nsteps) {
     for (auto& en : e->entries) cudaStreamWaitEvent(en.ctx->stream, e->ev1, 0);
     cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) return ens_fail(e, BFG_ECUDA, cudaGetErrorString(ce));
+    return 0;
+}
+
+int bfg_ens_autotune(bfg_ens* e, int reps) {
+    if (!e) return BFG_EINVAL;
+    if (reps < 1) reps = 1;
+    if (e->entries.empty()) return 0;
+    cudaSetDevice(e->device);
+    int rc = ens_prepare(e);
+    if (rc) return rc;
+    // the groups' streams follow everything the ensemble queued so far
+    if (cudaStreamSynchronize(e->stream) != cudaSuccess)
+        return ens_fail(e, BFG_ECUDA, "ensemble stream synchronisation failed");
+    for (EnsGroup* g : e->groups) {
+        double ms[2 * BFG_NKINDS] = {0};
+        rc = e->real_bytes == 4 ? ens_group_tune<float>(g, reps, ms) : ens_group_tune<double>(g, reps, ms);
+        if (rc) return ens_fail(e, rc, g->launcher.err.c_str());
+        tune_store(e->device, g->n, e->real_bytes, (int)g->members.size(), ms);
+    }
+    // captured graphs hold the old schedules: rebuild them before the next step
+    e->dirty = true;
     return 0;
 }
 

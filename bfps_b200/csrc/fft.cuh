@@ -144,15 +144,12 @@ __host__ __device__ constexpr int plan_radix(int L, int s, int MR) {
 __host__ __device__ constexpr int plan_block(int L, int s, int MR) {
     return s == 0 ? L : plan_block(L / plan_step(L, MR), s - 1, MR);
 }
-// radix cap of a strided-axis transform: up to 32 in FP32 for the passes
-// that gain from fewer stages (chosen per pass in passes.cuh), 8 in FP64
-// (twice the registers per value)
-#ifndef BFG_COL_MR_F32
-#define BFG_COL_MR_F32 32
-#endif
+// radix cap of a strided-axis transform: 32 in FP32 where the schedule asks
+// for wide butterflies, 8 otherwise and always in FP64 (twice the registers
+// per value)
 template <typename T, bool WIDE>
 __host__ __device__ constexpr int col_max_radix() {
-    return (sizeof(T) == 4 && WIDE) ? BFG_COL_MR_F32 : 8;
+    return (sizeof(T) == 4 && WIDE) ? 32 : 8;
 }
 
 // position of frequency k after a DIF of length L

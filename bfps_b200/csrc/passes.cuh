@@ -97,22 +97,21 @@ __host__ __device__ constexpr int pow2floor(int v) {
 }
 constexpr int SMEM_BUDGET = 220 * 1024;  // dynamic shared memory per SM we plan for
 __host__ __device__ constexpr bool col_fz(int mode) { return mode >= 5 && mode <= 7; }
-// Radix cap per pass (FP32): 32-point butterflies (two stages at 512^3
-// instead of three) in every column pass; with the two-CTA launch shape
-// below they measured faster for all of them (IZ 1.49 -> 1.33, IY 1.79 ->
-// 1.60, FY 0.88 -> 0.75 ms at 512^3).  A cap of 16 measured slower
-// everywhere.
-#ifndef BFG_FZ_WIDE
-#define BFG_FZ_WIDE 1
-#endif
-#ifndef BFG_Y_WIDE
-#define BFG_Y_WIDE 1
-#endif
-template <typename T, int MODE>
+// Schedules of a column pass.  Each pass is compiled in two schedules and
+// the one used is chosen per (device, grid size, precision, pass) by the
+// autotuner (bfg_autotune), schedule 0 where nothing was tuned:
+//   0: two 256-thread CTAs per SM with one tile buffer each (one CTA's
+//      barrier waits, loads and epilogue are covered by the other CTA's
+//      work), 32-point butterflies in FP32 (two stages at 512^3 instead of
+//      three);
+//   1: one 512-thread CTA per SM with two tile buffers (the next tile loads
+//      while this one is transformed), radix cap 8.
+// Measured at 512^3 FP32, schedule 0 against 1: IZ 1.33 / 1.49, IY 1.60 /
+// 1.79, FY 0.75 / 0.88, FZ 1.86 / 2.07 ms.  FP64 keeps a radix cap of 8 in
+// both (twice the registers per value).
+template <typename T, int MODE, int S>
 __host__ __device__ constexpr int col_mr() {
-    return col_max_radix<T, (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U ||
-                             (BFG_FZ_WIDE && MODE >= CM_FZ_RK1 && MODE <= CM_FZ_PLAIN) ||
-                             (BFG_Y_WIDE && (MODE == CM_Y_INV2 || MODE == CM_Y_FWD1)))>();
+    return col_max_radix<T, S == 0>();
 }
 
 // tile row pitch (complex) for a tile of TKX kx columns: keeps every row
@@ -129,12 +128,9 @@ __host__ __device__ constexpr int col_pitch_for(int tkx) {
 __host__ __device__ constexpr int col_nrk(int mode) {
     return mode == CM_FZ_RK1 ? 1 : ((mode == CM_FZ_RK2 || mode == CM_FZ_RK3) ? 2 : 0);
 }
-// Launch shape of a column pass.  Two 256-thread CTAs per SM with one tile
-// buffer each, where such a tile still has rows of at least 96 bytes: one
-// CTA's barrier waits, loads and (FZ) epilogue are covered by the other
-// CTA's work.  Otherwise one 512-thread CTA per SM with two tile buffers,
-// the next tile loading while this one is transformed.  Three CTAs per SM
-// for the one-buffer passes measured slower (FY 0.75 -> 1.03 ms).
+// Launch shape of a column pass (its schedule, above): schedule 0 runs two
+// CTAs per SM where such a tile still has rows of at least 96 bytes, else
+// one CTA with two buffers.
 // shared memory: nbuf tile buffers + twiddles
 template <typename T, int N, int MODE>
 __host__ __device__ constexpr size_t col_bytes_nb(int tkx, int nbuf) {
@@ -155,46 +151,28 @@ __host__ __device__ constexpr int col_tkx_sel(int nbuf, size_t budget) {
                ? N / 2 + 1
                : col_tkx_fit<T, N, MODE>(16, nbuf, budget);
 }
-// Measured at 512^3 FP32: FZ 2.06 -> 1.86 ms, IY 1.79 -> 1.60 ms (with the
-// radix cap of 32), against one 512-thread CTA with two buffers.
-#ifndef BFG_FZ_TWO
-#define BFG_FZ_TWO 1
-#endif
-#ifndef BFG_Y_TWO
-#define BFG_Y_TWO 1
-#endif
-template <typename T, int N, int MODE>
+template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr bool col_two() {
-    return (MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U ||
-            (BFG_FZ_TWO && MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) ||
-            (BFG_Y_TWO && (MODE == CM_Y_INV2 || MODE == CM_Y_FWD1))) &&
-           col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / 2) * 3 * (int)sizeof(cpx<T>) >= 96;
+    return S == 0 && col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / 2) * 3 * (int)sizeof(cpx<T>) >= 96;
 }
-// CTAs per SM of the single-buffer launch shape for the passes with one
-// buffer per tile (FY, FZ)
-#ifndef BFG_NB1_CTAS
-#define BFG_NB1_CTAS 2
-#endif
-template <typename T, int N, int MODE>
-__host__ __device__ constexpr int col_threads() { return col_two<T, N, MODE>() ? 256 : 512; }
-template <typename T, int N, int MODE>
-__host__ __device__ constexpr int col_ctas() {
-    return col_two<T, N, MODE>() ? (col_nb(MODE) == 1 ? BFG_NB1_CTAS : 2) : 1;
-}
-template <typename T, int N, int MODE>
-__host__ __device__ constexpr int col_nbuf() { return col_two<T, N, MODE>() ? 1 : 2; }
-template <typename T, int N, int MODE>
+template <typename T, int N, int MODE, int S>
+__host__ __device__ constexpr int col_threads() { return col_two<T, N, MODE, S>() ? 256 : 512; }
+template <typename T, int N, int MODE, int S>
+__host__ __device__ constexpr int col_ctas() { return col_two<T, N, MODE, S>() ? 2 : 1; }
+template <typename T, int N, int MODE, int S>
+__host__ __device__ constexpr int col_nbuf() { return col_two<T, N, MODE, S>() ? 1 : 2; }
+template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr int col_tkx() {
-    return col_two<T, N, MODE>() ? col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / col_ctas<T, N, MODE>())
+    return col_two<T, N, MODE, S>() ? col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / col_ctas<T, N, MODE, S>())
                                  : col_tkx_sel<T, N, MODE>(2, SMEM_BUDGET);
 }
-template <typename T, int N, int MODE>
+template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr int col_pitch() {
-    return col_pitch_for<T, col_nb(MODE)>(col_tkx<T, N, MODE>());
+    return col_pitch_for<T, col_nb(MODE)>(col_tkx<T, N, MODE, S>());
 }
-template <typename T, int N, int MODE>
+template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr size_t col_smem_bytes() {
-    return col_bytes_nb<T, N, MODE>(col_tkx<T, N, MODE>(), col_nbuf<T, N, MODE>());
+    return col_bytes_nb<T, N, MODE>(col_tkx<T, N, MODE, S>(), col_nbuf<T, N, MODE, S>());
 }
 
 template <int N>
@@ -289,7 +267,7 @@ __device__ __forceinline__ FzCol<T> fz_col(const KParams& kp, const T* __restric
     return fc;
 }
 
-template <typename T, int N, int MODE>
+template <typename T, int N, int MODE, int S>
 __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, int PR, int a, int l,
                                          int ix, int col, const FzCol<T>& fc, const cpx<T>* v0,
                                          const cpx<T>* vp, size_t pt, const T* __restrict__ filt,
@@ -299,7 +277,7 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     const double kz = kwrap<N>(l, kp.dkz);
     const double kx = fc.kx, ky = fc.ky;
     const double k2 = fc.kxy2 + kz * kz;
-    const int p = dif_position<N, col_mr<T, MODE>()>(l);
+    const int p = dif_position<N, col_mr<T, MODE, S>()>(l);
     cpx<T> nl[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) nl[c] = tile[p * PR + col * 3 + c];
@@ -380,20 +358,20 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     for (int c = 0; c < 3; ++c) out0[pt * 3 + c] = o[c];
 }
 
-template <typename T, int N, int MODE>
+template <typename T, int N, int MODE, int S>
 __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
                                                const cpx<T>* in1, int a, int kx0, int ncol,
                                                size_t nxp3, int tid) {
     constexpr int NB = col_nb(MODE);
     constexpr int NBIN = col_nbin(MODE);
-    constexpr int TKX = col_tkx<T, N, MODE>();
+    constexpr int TKX = col_tkx<T, N, MODE, S>();
     constexpr int W = 3 * TKX;
-    constexpr int PR = col_pitch<T, N, MODE>();
+    constexpr int PR = col_pitch<T, N, MODE, S>();
     constexpr int VB = ((W * (int)sizeof(cpx<T>)) % 16 == 0) ? 16 : 8;
     constexpr int VPE = VB / (int)sizeof(cpx<T>) > 0 ? VB / (int)sizeof(cpx<T>) : 1;  // complex per copy
     constexpr int WV = W / VPE;
     const int nvalid = (3 * ncol + VPE - 1) / VPE;
-    for (int e = tid; e < N * NBIN * WV; e += col_threads<T, N, MODE>()) {
+    for (int e = tid; e < N * NBIN * WV; e += col_threads<T, N, MODE, S>()) {
         const int v = e % WV;
         const int r = e / WV;
         const int b = r % NBIN;
@@ -433,15 +411,15 @@ __device__ __forceinline__ void tile_tickets_done(int* tctr, int tid) {
 // positions holds frequencies f(b) + (N/R) q; lanes take consecutive pencils,
 // i.e. consecutive complex numbers of one output row chunk.  NYQ: the tile
 // holds the Nyquist column only and PP counts its pencils (3 per buffer).
-template <typename T, int N, int MODE, int PP, bool NYQ>
+template <typename T, int N, int MODE, int S, int PP, bool NYQ>
 __device__ __forceinline__ void col_last_store(const cpx<T>* tile, int tid, const Member<T>& mb,
                                                const Roles& rl, int a, int kx0, int ncol) {
-    constexpr int NT = col_threads<T, N, MODE>();
-    constexpr int TKX = col_tkx<T, N, MODE>();
+    constexpr int NT = col_threads<T, N, MODE, S>();
+    constexpr int TKX = col_tkx<T, N, MODE, S>();
     constexpr int W = 3 * TKX;
-    constexpr int PR = col_pitch<T, N, MODE>();
+    constexpr int PR = col_pitch<T, N, MODE, S>();
     constexpr bool INV = col_inverse(MODE);
-    constexpr int MR = col_mr<T, MODE>();
+    constexpr int MR = col_mr<T, MODE, S>();
     constexpr int NST = plan_nstages(N, MR);
     constexpr int R = plan_radix(N, NST - 1, MR);
     constexpr int NW = PP * (N / R);
@@ -464,16 +442,16 @@ __device__ __forceinline__ void col_last_store(const cpx<T>* tile, int tid, cons
     }
 }
 
-template <typename T, int N, int MODE>
-__global__ void __launch_bounds__(col_threads<T, N, MODE>(), col_ctas<T, N, MODE>())
+template <typename T, int N, int MODE, int S>
+__global__ void __launch_bounds__(col_threads<T, N, MODE, S>(), col_ctas<T, N, MODE, S>())
 col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __restrict__ tw_g,
          int ntx, int tiles_per, int ntiles, int* __restrict__ tctr) {
-    constexpr int NT = col_threads<T, N, MODE>();
-    constexpr int NBUF = col_nbuf<T, N, MODE>();
+    constexpr int NT = col_threads<T, N, MODE, S>();
+    constexpr int NBUF = col_nbuf<T, N, MODE, S>();
     constexpr int NB = col_nb(MODE);
-    constexpr int TKX = col_tkx<T, N, MODE>();
+    constexpr int TKX = col_tkx<T, N, MODE, S>();
     constexpr int W = 3 * TKX;                     // complex per row per buffer
-    constexpr int PR = col_pitch<T, N, MODE>();    // tile row pitch
+    constexpr int PR = col_pitch<T, N, MODE, S>();    // tile row pitch
     constexpr int TILE = N * PR;
     constexpr bool INV = col_inverse(MODE);
     constexpr int VB = ((W * (int)sizeof(cpx<T>)) % 16 == 0) ? 16 : 8;
@@ -504,7 +482,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     if (t < ntiles) {
         const int m = t / tiles_per, tl = t - m * tiles_per;
         const int kx0 = (tl % ntx) * TKX;
-        col_issue_load<T, N, MODE>(bufs, mbuf(mem[m], rl.in0), mbuf(mem[m], rl.in1), tl / ntx, kx0,
+        col_issue_load<T, N, MODE, S>(bufs, mbuf(mem[m], rl.in0), mbuf(mem[m], rl.in1), tl / ntx, kx0,
                                    min(TKX, NXV - kx0), nxp3, tid);
     }
     cp_async_commit();
@@ -544,7 +522,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             if (tn < ntiles) {
                 const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
                 const int kx0n = (tln % ntx) * TKX;
-                col_issue_load<T, N, MODE>(bufs + ((it + 1) & 1) * TILE, mbuf(mem[mn], rl.in0),
+                col_issue_load<T, N, MODE, S>(bufs + ((it + 1) & 1) * TILE, mbuf(mem[mn], rl.in0),
                                            mbuf(mem[mn], rl.in1), tln / ntx, kx0n,
                                            min(TKX, NXV - kx0n), nxp3, tid);
             }
@@ -631,7 +609,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         // the tile holding only the Nyquist column transforms just its pencils
         using LYN = Lay<3, W, 1, PR>;
         constexpr int PN = NB * 3;
-        constexpr int MR = col_mr<T, MODE>();
+        constexpr int MR = col_mr<T, MODE, S>();
         constexpr int NST = plan_nstages(N, MR);
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
             if (ncol == TKX) dif<T, N, INV, P, LY, 1, N, MR>(tile, tw, tid, NT);
@@ -643,7 +621,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 const size_t pt = ((size_t)a * N + l) * (N / 2 + 4) + kx0 + col;  // S[ky=a][kz=l][kx]
                 const cpx<T>* v0 = mbuf(mb, rl.v0) + pt * 3;
                 const cpx<T>* vp = NRK > 1 ? mbuf(mb, rl.vp) + pt * 3 : v0;
-                fz_point<T, N, MODE>(kp, tile, PR, a, l, kx0 + col, col, fc, v0, vp, pt, mb.filt,
+                fz_point<T, N, MODE, S>(kp, tile, PR, a, l, kx0 + col, col, fc, v0, vp, pt, mb.filt,
                                      mb.fac, mbuf(mb, rl.fsrc), mbuf(mb, rl.out0));
             };
             if constexpr (NT % TKX == 0) {
@@ -664,10 +642,10 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         } else {
             if (ncol == TKX) {
                 dif_range<T, N, 0, NST - 1, INV, P, LY, 1, N, MR>(tile, tw, tid, NT);
-                col_last_store<T, N, MODE, P, false>(tile, tid, mb, rl, a, kx0, ncol);
+                col_last_store<T, N, MODE, S, P, false>(tile, tid, mb, rl, a, kx0, ncol);
             } else {
                 dif_range<T, N, 0, NST - 1, INV, PN, LYN, 1, N, MR>(tile, tw, tid, NT);
-                col_last_store<T, N, MODE, PN, true>(tile, tid, mb, rl, a, kx0, ncol);
+                col_last_store<T, N, MODE, S, PN, true>(tile, tid, mb, rl, a, kx0, ncol);
             }
         }
         __syncthreads();  // this buffer is refilled by the next load
@@ -676,7 +654,7 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             if (tn < ntiles) {
                 const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
                 const int kx0n = (tln % ntx) * TKX;
-                col_issue_load<T, N, MODE>(bufs, mbuf(mem[mn], rl.in0), mbuf(mem[mn], rl.in1),
+                col_issue_load<T, N, MODE, S>(bufs, mbuf(mem[mn], rl.in0), mbuf(mem[mn], rl.in1),
                                            tln / ntx, kx0n, min(TKX, NXV - kx0n), nxp3, tid);
             }
             cp_async_commit();

@@ -182,6 +182,30 @@ class vorticity_equation:
         check(lib().bfg_check_finite(self._h, fid, ctypes.byref(n)), self._h)
         return n.value
 
+    def autotune(self, reps=3):
+        """bfg_autotune: time both schedules of the IZ, IY, FY and FZ passes
+        on this context and keep the faster for this device, grid size and
+        precision, one member per launch.  Returns {pass: (schedule, ms0,
+        ms1)}.  The context's velocity fields are used as work space
+        (recompute them afterwards)."""
+        check(lib().bfg_autotune(self._h, int(reps)), self._h)
+        return self.schedules()
+
+    def schedules(self, members=1):
+        """{pass: (schedule, ms0, ms1)} for launches over `members` contexts
+        of this grid size and precision (ensemble groups of that size)."""
+        out = {}
+        for kind, name in ((0, "IZ"), (1, "IY"), (3, "FY"), (4, "FZ")):
+            sc, m0, m1 = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+            check(lib().bfg_tune_get(self._h, kind, int(members), ctypes.byref(sc),
+                                     ctypes.byref(m0), ctypes.byref(m1)), self._h)
+            out[name] = (sc.value, m0.value, m1.value)
+        return out
+
+    def set_schedule(self, name, schedule, members=1):
+        kind = {"IZ": 0, "IY": 1, "FY": 3, "FZ": 4}[name]
+        check(lib().bfg_tune_set(self._h, kind, int(members), int(schedule)), self._h)
+
     def last_step_ms(self):
         ms = ctypes.c_double()
         check(lib().bfg_last_step_ms(self._h, ctypes.byref(ms)), self._h)
@@ -311,6 +335,16 @@ class ensemble:
 
     def use_graphs(self, enable):
         self._check(lib().bfg_ens_use_graphs(self._h, int(bool(enable))))
+
+    def autotune(self, reps=3):
+        """bfg_ens_autotune: both column-pass schedules timed on every size
+        group as step() launches it.  Returns {N: {pass: (schedule, ms0,
+        ms1)}}.  The members' velocity fields are used as work space."""
+        self._check(lib().bfg_ens_autotune(self._h, int(reps)))
+        groups = {}
+        for fs, _, _ in self.members:
+            groups.setdefault(fs.nx, []).append(fs)
+        return {n: fss[0].schedules(members=len(fss)) for n, fss in groups.items()}
 
     def wait(self, timeout_s=None):
         """True once the last step() call's work has finished; False if it

@@ -254,6 +254,32 @@ int bfg_last_step_ms(bfg_ctx* ctx, double* ms);
 int bfg_profile(bfg_ctx* ctx, int enable);
 int bfg_profile_read(bfg_ctx* ctx, int kind, double* total_ms, int64_t* launches);
 
+/* Autotuner of the column passes (no counterpart in the reference, whose
+ * FFTW plans are chosen by FFTW's own planner rigor, bfps/cpp/
+ * fftw_interface.hpp:30-35).  Every pass over z or y (kinds 0 IZ, 1 IY,
+ * 3 FY, 4 FZ) is built in two schedules: 0, two 256-thread CTAs per SM with
+ * one tile buffer each and 32-point butterflies in FP32; 1, one 512-thread
+ * CTA with two tile buffers and radix-8 butterflies.  The choice is kept per
+ * device, grid size, precision and members per launch (1 for a lone
+ * context; the size of an ensemble's group of equal grids otherwise), since
+ * the better schedule depends on how many tiles one launch holds.
+ * bfg_autotune times both on this context's buffers (reps launches each,
+ * after one warm-up; only the work buffers are written, so the complex and
+ * real velocity of the context are lost) for one member per launch.
+ * bfg_ens_autotune does the same for every size group of an ensemble, as
+ * bfg_ens_step launches it (all members of the group in one launch), and
+ * re-captures the ensemble's graphs at its next step.  Schedule 1 is chosen
+ * only when it is more than 2% faster than schedule 0.  Where the environment
+ * variable BFPS_B200_TUNE_CACHE names a file, the choices are appended to it
+ * and read back by later processes on a device of the same name.  A key
+ * never tuned uses schedule 0.  bfg_tune_get reads the choice for a member
+ * count and its measured times (0 when not measured), bfg_tune_set imposes
+ * one. */
+int bfg_autotune(bfg_ctx* ctx, int reps);
+int bfg_ens_autotune(bfg_ens* e, int reps);
+int bfg_tune_get(const bfg_ctx* ctx, int kind, int members, int* schedule, double* ms0, double* ms1);
+int bfg_tune_set(bfg_ctx* ctx, int kind, int members, int schedule);
+
 /* Count of kernels the library launched since the context was created. */
 int bfg_kernel_launches(const bfg_ctx* ctx, int64_t* count);
 
