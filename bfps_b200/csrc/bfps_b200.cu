@@ -183,7 +183,7 @@ struct Prof {
 static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 
 // A kernel whose bounded wait on its own bulk copies ran out sets
-// g_bfg_wait_status (xpass.cuh); read (and cleared) after the work is done.
+// g_bfg_wait_status (bulk.cuh); read (and cleared) after the work is done.
 static int check_wait_status(bfg_ctx* c) {
     int st = 0;
     CU(cudaMemcpyFromSymbol(&st, g_bfg_wait_status, sizeof(int)));
@@ -1332,6 +1332,28 @@ int bfg_set_iteration(bfg_ctx* c, int it) {
     if (!c) return BFG_EINVAL;
     c->iteration = it;
     return 0;
+}
+
+// bfg_selftest_wait: one warp waits on an mbarrier that nothing arms, with
+// a short bound, so the wait runs out and sets the status word
+__global__ void wait_selftest_kernel(unsigned limit) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    mbar_wait_bounded(&bar, 0, limit);
+}
+
+int bfg_selftest_wait(bfg_ctx* c) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    CU(cudaStreamSynchronize(c->stream));
+    wait_selftest_kernel<<<1, 32, 0, c->stream>>>(1u << 12);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(c->stream));
+    return check_wait_status(c);
 }
 
 int bfg_last_step_ms(bfg_ctx* c, double* ms) {

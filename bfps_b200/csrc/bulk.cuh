@@ -48,8 +48,9 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 }
 // bounded wait for phase `parity` of bar; false (and the status word set)
 // if the copies have not landed after the limit
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (unsigned i = 0; i < (1u << 22); ++i)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned limit = 1u << 22) {
+    for (unsigned i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     atomicExch(&g_bfg_wait_status, 1);
     return false;

@@ -280,6 +280,16 @@ int bfg_ens_autotune(bfg_ens* e, int reps);
 int bfg_tune_get(const bfg_ctx* ctx, int kind, int members, int* schedule, double* ms0, double* ms1);
 int bfg_tune_set(bfg_ctx* ctx, int kind, int members, int schedule);
 
+/* No counterpart in the reference: exercises the error path of the
+ * library's bounded waits.  Kernels that wait on their own TMA bulk copies
+ * (mbarrier waits) give up after a bound, set a device status word and
+ * return; the next synchronising call (bfg_last_step_ms, a download) reads
+ * the word and fails with BFG_ECUDA and a message.  This call launches one
+ * warp whose wait, on an mbarrier that nothing arms, runs out after a short
+ * bound, and returns what that check reports: BFG_ECUDA, with the status
+ * word cleared and the context still usable. */
+int bfg_selftest_wait(bfg_ctx* ctx);
+
 /* Count of kernels the library launched since the context was created. */
 int bfg_kernel_launches(const bfg_ctx* ctx, int64_t* count);
 
