@@ -1251,10 +1251,21 @@ static bool is_host_memory(const void* p) {
     return at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged;
 }
 
+// Caller buffers in device memory may still be written (or read) by work
+// the caller queued on other streams; the library's streams do not wait
+// for the legacy default stream, so a call that takes such a buffer first
+// waits for all work queued on the device.
+static int order_after_caller(bfg_ctx* c, const void* a, const void* b) {
+    if (is_host_memory(a) && (!b || is_host_memory(b))) return 0;
+    CU(cudaDeviceSynchronize());
+    return 0;
+}
+
 int bfg_ift(bfg_ctx* c, const void* din, void* dout) {
     if (!c || !din || !dout) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
     if (int rj = join_tracers(c)) return rj;
+    if (int ro = order_after_caller(c, din, dout)) return ro;
     int rc = ensure_ru(c);
     if (rc) return rc;
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
@@ -1278,6 +1289,7 @@ int bfg_dft(bfg_ctx* c, const void* din, void* dout) {
     if (!c || !din || !dout) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
     if (int rj = join_tracers(c)) return rj;
+    if (int ro = order_after_caller(c, din, dout)) return ro;
     int rc = ensure_ru(c);
     if (rc) return rc;
     const size_t N = c->n, cb = 2 * (size_t)c->real_bytes, rb = c->real_bytes;
@@ -1313,6 +1325,7 @@ int bfg_field_stats(bfg_ctx* c, const void* field, double max_estimate, int nbin
     if (!c || !field || nbins < 1) return BFG_EINVAL;
     CU(cudaSetDevice(c->device));
     if (int rj = join_tracers(c)) return rj;
+    if (int ro = order_after_caller(c, field, nullptr)) return ro;
     int rc = sync_member(c, c->fac_dt);
     if (rc) return rc;
     // into v1 (free between steps), re-pitched to the device rows

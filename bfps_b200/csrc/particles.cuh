@@ -17,6 +17,7 @@
 // kernel overwrites it instead of accumulating (accum = false).
 #pragma once
 #include <stdint.h>
+#include <type_traits>
 #include "interp_coeffs.h"
 
 namespace bfg {
@@ -181,32 +182,36 @@ __device__ __forceinline__ double group_sum(double v, unsigned gmask) {
 // aligned-down start belongs to point (i - off) / 3, component
 // (i - off) mod 3, so each lane's x weights are shifted once per tracer and its
 // sums are kept per word phase i mod 3, mapped to components at the end.
+#ifndef BFG_TRACER_ROWSUM_F64
+#define BFG_TRACER_ROWSUM_F64 0
+#endif
 template <int NB, int L>
 __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int N, const int* g,
                                                int x0, const double* wx, const double* wy,
                                                const double* wz, int j, unsigned gmask,
                                                double& a0, double& a1, double& a2) {
+    using SumT = typename std::conditional<BFG_TRACER_ROWSUM_F64 != 0, double, float>::type;
     constexpr int NP = 2 * NB + 2;
     constexpr int VW = 8;                                // floats per vector
     constexpr int NVMAX = (3 * NP + 2 * (VW - 1)) / VW;  // vectors covering any alignment
     constexpr int VPL = (NVMAX + L - 1) / L;             // vectors per lane
     const size_t rowN = (size_t)N;
-    float wxf[NP];
+    SumT wxf[NP];
 #pragma unroll
-    for (int ix = 0; ix < NP; ++ix) wxf[ix] = (float)wx[ix];
+    for (int ix = 0; ix < NP; ++ix) wxf[ix] = (SumT)wx[ix];
     if (x0 >= 0 && x0 + NP <= N) {
         const int e0 = x0 * 3;
         const int base = e0 & ~(VW - 1);
         const int off = e0 - base;
         // vectors holding stencil words, none past the end of the row
         const int nv = min((off + 3 * NP + VW - 1) / VW, (N * 3 - base) / VW);
-        float wl[VPL][VW];
+        SumT wl[VPL][VW];
 #pragma unroll
         for (int t = 0; t < VPL; ++t)
 #pragma unroll
             for (int u = 0; u < VW; ++u) {
                 const int k = VW * (j + L * t) + u - off;  // 3 * point + component
-                float w = 0.f;
+                SumT w = 0;
 #pragma unroll
                 for (int pt = 0; pt < NP; ++pt) w = (k >= 3 * pt && k < 3 * pt + 3) ? wxf[pt] : w;
                 wl[t][u] = w;
@@ -224,7 +229,7 @@ __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int
                 const int y = wrap_once(g[1] - NB + iy, N);
                 const float* row = ru + ((size_t)z * rowN + y) * rowN * 3 + base;
                 const double bzy = bz * wy[iy];
-                float sp[3] = {0.f, 0.f, 0.f};
+                SumT sp[3] = {0, 0, 0};
 #pragma unroll
                 for (int t = 0; t < VPL; ++t) {
                     if (j + L * t < nv) {
@@ -232,7 +237,7 @@ __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int
                         ld_v8(row + VW * (j + L * t), q);
 #pragma unroll
                         for (int u = 0; u < VW; ++u)
-                            sp[(2 * L * t + u) % 3] = fmaf(q[u], wl[t][u], sp[(2 * L * t + u) % 3]);
+                            sp[(2 * L * t + u) % 3] = fma((SumT)q[u], wl[t][u], sp[(2 * L * t + u) % 3]);
                     }
                 }
 #pragma unroll
@@ -254,12 +259,12 @@ __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int
         // stencil across the periodic x boundary: lane j takes the points
         // ix = j, j + L, ... with scalar loads
         constexpr int PPL = (NP + L - 1) / L;  // points per lane
-        float wj[PPL];
+        SumT wj[PPL];
         int xj[PPL];
 #pragma unroll
         for (int m = 0; m < PPL; ++m) {
             const int ix = j + L * m;
-            float w = 0.f;
+            SumT w = 0;
 #pragma unroll
             for (int pt = 0; pt < NP; ++pt) w = ix == pt ? wxf[pt] : w;
             wj[m] = w;
@@ -274,13 +279,13 @@ __device__ __forceinline__ void row_gather_f32(const float* __restrict__ ru, int
             for (int iy = 0; iy < NP; ++iy) {
                 const int y = wrap_once(g[1] - NB + iy, N);
                 const float* row = ru + ((size_t)z * rowN + y) * rowN * 3;
-                float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+                SumT s0 = 0, s1 = 0, s2 = 0;
 #pragma unroll
                 for (int m = 0; m < PPL; ++m) {
                     if (xj[m] >= 0) {
-                        s0 = fmaf(row[xj[m] * 3 + 0], wj[m], s0);
-                        s1 = fmaf(row[xj[m] * 3 + 1], wj[m], s1);
-                        s2 = fmaf(row[xj[m] * 3 + 2], wj[m], s2);
+                        s0 = fma((SumT)row[xj[m] * 3 + 0], wj[m], s0);
+                        s1 = fma((SumT)row[xj[m] * 3 + 1], wj[m], s1);
+                        s2 = fma((SumT)row[xj[m] * 3 + 2], wj[m], s2);
                     }
                 }
                 const double bzy = bz * wy[iy];

@@ -159,12 +159,17 @@ template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr int col_threads() { return col_two<T, N, MODE, S>() ? 256 : 512; }
 template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr int col_ctas() { return col_two<T, N, MODE, S>() ? 2 : 1; }
+// From 1024-point columns up, schedule 1 keeps one buffer: two buffers of
+// such columns leave tiles of one or two kx columns (24-48-byte row
+// segments), one buffer twice or four times as wide.
 template <typename T, int N, int MODE, int S>
-__host__ __device__ constexpr int col_nbuf() { return col_two<T, N, MODE, S>() ? 1 : 2; }
+__host__ __device__ constexpr int col_nbuf() {
+    return col_two<T, N, MODE, S>() ? 1 : ((S == 1 && N >= 1024) ? 1 : 2);
+}
 template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr int col_tkx() {
     return col_two<T, N, MODE, S>() ? col_tkx_sel<T, N, MODE>(1, SMEM_BUDGET / col_ctas<T, N, MODE, S>())
-                                 : col_tkx_sel<T, N, MODE>(2, SMEM_BUDGET);
+                                 : col_tkx_sel<T, N, MODE>(col_nbuf<T, N, MODE, S>(), SMEM_BUDGET);
 }
 template <typename T, int N, int MODE, int S>
 __host__ __device__ constexpr int col_pitch() {

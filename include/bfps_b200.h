@@ -118,7 +118,10 @@ int bfg_lagrangian_acceleration(bfg_ctx* ctx, void* host);
 /* field::ift / field::dft (field.cpp:144-162) on a 3-vector field, using
  * caller device buffers in the reference layouts (complex: (n, n, n/2+1, 3),
  * real: (n, n, n+2, 3)); unnormalised like FFTW.  in may equal out; host
- * or device memory (unified addressing). */
+ * or device memory (unified addressing).  Where either buffer is device
+ * memory the call first waits for all work queued on the device (the
+ * caller's kernels on any stream), and it returns once the output is
+ * complete. */
 int bfg_ift(bfg_ctx* ctx, const void* dev_complex_in, void* dev_real_out);
 int bfg_dft(bfg_ctx* ctx, const void* dev_real_in, void* dev_complex_out);
 
@@ -133,7 +136,8 @@ int bfg_field_ift(bfg_ctx* ctx, int field_id);
  * co-spectrum (nshells, 3, 3), real-space moments (10, 4) and histograms
  * (nbins, 4) with max_estimate per component (max_estimate sqrt(3) for the
  * magnitude, field.cpp:1001-1004).  Uses the context's free RK buffer; the
- * state and the velocity are untouched.  Outputs may be NULL. */
+ * state and the velocity are untouched.  Outputs may be NULL.  A field in
+ * device memory is read after all work queued on the device. */
 int bfg_field_stats(bfg_ctx* ctx, const void* field, double max_estimate, int nbins,
                     double* spec, double* mom, int64_t* hist);
 
