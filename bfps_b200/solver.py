@@ -11,12 +11,30 @@ the reference's host layouts (bfps/cpp/field.cpp:85-101).
 
 All compute runs in the CUDA library; every method raises on failure.
 """
+import atexit
 import ctypes
+import weakref
 
 import numpy as np
 
 from . import _lib
 from ._lib import check, lib, ptr
+
+# Objects still open when the interpreter exits are closed here, before the
+# modules are torn down, ensembles first, then tracer sets, then their
+# contexts (a tracer set's destruction synchronises its context's streams).
+_live = {"ensemble": weakref.WeakSet(), "particles": weakref.WeakSet(),
+         "context": weakref.WeakSet()}
+
+
+@atexit.register
+def _close_all():
+    for kind in ("ensemble", "particles", "context"):
+        for obj in list(_live[kind]):
+            try:
+                obj.close()
+            except Exception:
+                pass
 
 
 class vorticity_equation:
@@ -35,6 +53,7 @@ class vorticity_equation:
             raise _lib.BfgError(rc, "bfg_ctx_create(%d, %d, %d, precision=%s)" %
                                 (nx, ny, nz, precision))
         self._h = h
+        _live["context"].add(self)
         # defaults of the reference constructor (vorticity_equation.cpp:150-155)
         self._nu = 0.1
         self._forcing_type = "none"
@@ -244,6 +263,7 @@ class particles_system:
                                          nsteps, ptr(pos), ptr(rhs), ptr(idx, ctypes.c_int64),
                                          step_idx), fs.handle)
         self._h = h
+        _live["particles"].add(self)
         self.fs = fs
         self.n = n
         self.nsteps = nsteps
@@ -310,6 +330,7 @@ class ensemble:
         h = ctypes.c_void_p()
         check(lib().bfg_ens_create(ctypes.byref(h), device))
         self._h = h
+        _live["ensemble"].add(self)
         self.members = []
 
     def _check(self, rc):
