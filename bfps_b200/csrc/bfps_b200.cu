@@ -301,15 +301,21 @@ static int tuned_schedule(int dev, int n, int rb, int kind, int nmem) {
     auto it = g_tune.find(TuneKey(dev, n, rb, kind, nmem));
     return it == g_tune.end() ? 0 : it->second.sched;
 }
-// Schedule 1 replaces the default only when it is faster by more than this
-// fraction: the tuner times one launch at a time, and schedule 0 (two CTAs
-// per SM) shares the SMs better with the concurrent launches of an
-// ensemble's other size groups, so near-ties go to it.
+// Schedule 1 replaces the default only when it is faster by more than a
+// margin: the tuner times one launch at a time, and schedule 0 (two CTAs per
+// SM) shares the SMs with concurrent launches, where schedule 1 (one CTA
+// holding all of an SM's shared memory) keeps every other launch off the
+// SMs it runs on.  Near-ties go to schedule 0 (2 %); for the size groups of
+// an ensemble that holds several sizes, whose launches run concurrently,
+// schedule 1 must be 10 % faster alone (measured on the C4 mix: choices
+// made at 2 % lost 1 % of the ensemble step).
 constexpr double TUNE_MARGIN = 0.02;
+constexpr double TUNE_MARGIN_SHARED = 0.10;
 
 // record measured times (ms[kind * 2 + schedule]) for nmem members per
 // launch, the chosen schedule, and append them to the cache file
-static void tune_store(int dev, int n, int rb, int nmem, const double* ms) {
+static void tune_store(int dev, int n, int rb, int nmem, const double* ms,
+                       double margin = TUNE_MARGIN) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tune_load_locked(dev);
     const char* path = std::getenv("BFPS_B200_TUNE_CACHE");
@@ -319,7 +325,7 @@ static void tune_store(int dev, int n, int rb, int nmem, const double* ms) {
         TuneEntry e;
         e.ms0 = ms[2 * kind];
         e.ms1 = ms[2 * kind + 1];
-        e.sched = e.ms1 < e.ms0 * (1.0 - TUNE_MARGIN) ? 1 : 0;
+        e.sched = e.ms1 < e.ms0 * (1.0 - margin) ? 1 : 0;
         g_tune[TuneKey(dev, n, rb, kind, nmem)] = e;
         if (f)
             std::fprintf(f, "%s %d %d %d %d %d %.6f %.6f\n", name.c_str(), n, rb, kind, nmem, e.sched,
@@ -423,6 +429,23 @@ struct Engine {
                 reinterpret_cast<const Member<float>*>(mem), rl,
                 reinterpret_cast<const cpx<float>*>(c->tw), rows_per, nrows);
             return after_launch(c, "row_nonlin_warp");
+        } else if constexpr (MODE == RM_NONLIN && sizeof(T) == 4 && (N == 64 || N == 128 || N == 256)) {
+            // FP32 64^3 - 256^3: warp-group x pass (xpass.cuh)
+            constexpr size_t smem = xwg_smem_bytes<N>();
+            auto kern = row_nonlin_wg<N, WRU>;
+            if (smem > (size_t)c->smem_optin)
+                return fail(c, BFG_EUNSUP, "x pass needs %zu bytes of shared memory", smem);
+            CU(ensure_smem(kern, smem, c->device));
+            constexpr int Q = xwg::Cfg<N>::Q;
+            const int rows_per = N * N;
+            const int nrows = rows_per * nmem;
+            const int nblk = nrows / Q;
+            const int grid = std::min(c->nsm, (nblk + xwg::NWARP - 1) / xwg::NWARP);
+            Prof pr(c, K_X);
+            kern<<<grid, xwg::NWARP * 32, smem, c->stream>>>(
+                reinterpret_cast<const Member<float>*>(mem), rl,
+                reinterpret_cast<const cpx<float>*>(c->tw), rows_per, nrows);
+            return after_launch(c, "row_nonlin_wg");
         } else if constexpr (MODE == RM_NONLIN && rnl_fused<T, N>()) {
             constexpr size_t smem = rnl_smem_bytes<T, N>();
             constexpr int ROWS = rnl_rows<T, N>();
@@ -2367,7 +2390,8 @@ int bfg_ens_autotune(bfg_ens* e, int reps) {
         double ms[2 * BFG_NKINDS] = {0};
         rc = e->real_bytes == 4 ? ens_group_tune<float>(g, reps, ms) : ens_group_tune<double>(g, reps, ms);
         if (rc) return ens_fail(e, rc, g->launcher.err.c_str());
-        tune_store(e->device, g->n, e->real_bytes, (int)g->members.size(), ms);
+        tune_store(e->device, g->n, e->real_bytes, (int)g->members.size(), ms,
+                   e->groups.size() > 1 ? TUNE_MARGIN_SHARED : TUNE_MARGIN);
     }
     // captured graphs hold the old schedules: rebuild them before the next step
     e->dirty = true;

@@ -273,7 +273,9 @@ int bfg_profile_read(bfg_ctx* ctx, int kind, double* total_ms, int64_t* launches
  * bfg_ens_autotune does the same for every size group of an ensemble, as
  * bfg_ens_step launches it (all members of the group in one launch), and
  * re-captures the ensemble's graphs at its next step.  Schedule 1 is chosen
- * only when it is more than 2% faster than schedule 0.  Where the environment
+ * only when it is more than 2% faster than schedule 0 (10% for the groups of
+ * an ensemble that holds several grid sizes, whose launches run
+ * concurrently: schedule 1 holds all of an SM's shared memory).  Where the environment
  * variable BFPS_B200_TUNE_CACHE names a file, the choices are appended to it
  * and read back by later processes on a device of the same name.  A key
  * never tuned uses schedule 0.  bfg_tune_get reads the choice for a member

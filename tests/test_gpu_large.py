@@ -131,3 +131,72 @@ def test_fp32_512_c3_step_against_fp64_oracle():
     # rhs[1] holds u(x(t)) after the history shift
     assert rel_err(rhs[1], wrhs[1]) < 1e-5
     assert np.abs(got - want).max() / (2 * np.pi) < 1e-9
+
+
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_fp32_step_64_to_256_against_fp64_oracle(n):
+    """One NSVEparticles step in FP32 at 64^3, 128^3 and 256^3, where the x
+    pass is the warp-group kernel (eight, four and two rows per warp), against the FP64
+    oracle from the same FP32-rounded field and tracers: the field within
+    2e-5 of max|w|, the sampled velocity (read from the real velocity the x
+    pass writes in stage 1) within 1e-5 of max|u|, positions within 1e-9 of
+    the box (vorticity_equation.cpp:358-439, NSVEparticles.cpp:33-41)."""
+    from bfps_b200.solver import vorticity_equation, particles_system, NSVEparticles_step
+    ntr, dt = 20000, 0.002
+    w0 = ic.vorticity_ic(n, seed=3, k0=4.0).astype(np.complex64)
+    pos = ic.tracer_ic(ntr, seed=4)
+    ve = vorticity_equation(n, precision="single")
+    ve.nu, ve.forcing_type, ve.famplitude, ve.fk0, ve.fk1 = 0.005, "linear", 0.5, 1.5, 3.0
+    ve.set_cvorticity(w0)
+    ps = particles_system(ve, pos, 3, 2, 3)
+    NSVEparticles_step(ve, ps, dt)
+    w_gpu = ve.get_cvorticity()
+    got, rhs, _ = ps.state()
+    ps.close()
+    ve.close()
+    ref = F.VorticityEquation(n)
+    ref.nu, ref.forcing_type, ref.famplitude, ref.fk0, ref.fk1 = 0.005, "linear", 0.5, 1.5, 3.0
+    ref.cvorticity = w0.astype(np.complex128)
+    rps = F.ParticlesSystem(ref, pos, np.zeros((3, ntr, 3)), 3, 2)
+    F.nsveparticles_step(ref, rps, dt)
+    want, wrhs, _ = rps.state()
+    rps.close()
+    w_ref = ref.cvorticity
+    ref.close()
+    assert rel_err(w_gpu, w_ref) < 2e-5
+    assert rel_err(rhs[1], wrhs[1]) < 1e-5
+    assert np.abs(got - want).max() / (2 * np.pi) < 1e-9
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_fp32_ensemble_equals_alone(n):
+    """Two FP32 members of one size in one ensemble (one x-pass launch over
+    both, row blocks numbered across members) give bit for bit what each
+    gives stepped alone."""
+    from bfps_b200.solver import vorticity_equation, particles_system, NSVEparticles_step, ensemble
+
+    def make(seed):
+        ve = vorticity_equation(n, precision="single")
+        ve.nu, ve.forcing_type, ve.famplitude, ve.fk0, ve.fk1 = 0.01 * seed, "linear", 0.5, 1.5, 3.0
+        ve.set_cvorticity(ic.vorticity_ic(n, seed=seed, k0=4.0).astype(np.complex64))
+        ps = particles_system(ve, ic.tracer_ic(5000, seed=seed), 2, 1, 3)
+        return ve, ps
+
+    mem = [make(1), make(2)]
+    alone = [make(1), make(2)]
+    ens = ensemble()
+    try:
+        for ve, ps in mem:
+            ens.add(ve, 0.002, ps)
+        ens.step(3)
+        for ve, ps in alone:
+            NSVEparticles_step(ve, ps, 0.002, 3)
+        for (a, pa), (b, pb) in zip(mem, alone):
+            assert np.array_equal(a.get_cvorticity(), b.get_cvorticity())
+            sa, sb = pa.state(), pb.state()
+            assert np.array_equal(sa[0], sb[0]) and np.array_equal(sa[1], sb[1])
+    finally:
+        ens.close()
+        for ve, ps in mem + alone:
+            ps.close()
+            ve.close()

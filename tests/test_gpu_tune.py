@@ -114,7 +114,8 @@ def test_ensemble_autotune_then_other_schedule_equals_alone(graphs):
         for n, t in tuned.items():
             for p in PASSES:
                 sched, ms0, ms1 = t[p]
-                assert ms0 > 0 and ms1 > 0 and sched == (1 if ms1 < ms0 * (1.0 - 0.02) else 0)
+                # two size groups: schedule 1 must win by 10 %
+                assert ms0 > 0 and ms1 > 0 and sched == (1 if ms1 < ms0 * (1.0 - 0.10) else 0)
         # the group launches (3 x 32^3, 2 x 16^3) switched to schedule 1; the
         # graphs are re-captured at the next step
         for n, k in counts.items():
