@@ -585,9 +585,13 @@ def run_serving(args, cfg):
     srv.done.clear()
     barrier(pg)
     launches0 = srv.ens.kernel_launches()
+    busy0, ticks0, host0 = srv.busy_ms, srv.ticks, dict(srv.host_s)
     t0 = time.perf_counter()
     done = srv.run(reqs)
     wall = time.perf_counter() - t0
+    busy_s = (srv.busy_ms - busy0) / 1e3
+    ticks = srv.ticks - ticks0
+    srv_host = {k: v - host0[k] for k, v in srv.host_s.items()}
     launches = srv.ens.kernel_launches() - launches0
     srv.close()
     ttc = np.array([r.finished - r.arrival for r in done])
@@ -619,7 +623,10 @@ def run_serving(args, cfg):
         "p50_s": round(float(np.percentile(ttc, 50)), 4),
         "p99_s": round(float(np.percentile(ttc, 99)), 4),
         "completed": len(done), "wall_s": round(wall, 3),
+        "device_busy_s": round(busy_s, 3), "ticks": ticks,
+        "host_phases_s": {k: round(v, 3) for k, v in srv_host.items()},
         "sequential": {"solves_s": round(seq_solves_s, 4), "speedup": round(solves_s / seq_solves_s, 3),
+                       "device_s": round(seq_s, 3),
                        "how": "sum of steps x single-instance step time per size"},
         "e2e": {"value": round(solves_s * world, 4), "unit": "solves/s",
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,

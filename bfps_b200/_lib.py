@@ -72,6 +72,7 @@ SIGNATURES = {
     "bfg_autotune": (_i, [_vp, _i]),
     "bfg_ens_autotune": (_i, [_vp, _i]),
     "bfg_selftest_wait": (_i, [_vp]),
+    "bfg_ctx_reset": (_i, [_vp]),
     "bfg_tune_get": (_i, [_vp, _i, _i, _c.POINTER(_i), _pd, _pd]),
     "bfg_tune_set": (_i, [_vp, _i, _i, _i]),
     "bfg_field_stats": (_i, [_vp, _vp, _d, _i, _pd, _pd, _pi64]),

@@ -1359,6 +1359,17 @@ int bfg_field_stats(bfg_ctx* c, const void* field, double max_estimate, int nbin
     return dispatch<OpStats>(c, (int)B_V1, max_estimate, nbins, spec, mom, hist);
 }
 
+int bfg_ctx_reset(bfg_ctx* c) {
+    if (!c) return BFG_EINVAL;
+    CU(cudaSetDevice(c->device));
+    if (int rj = join_tracers(c)) return rj;
+    for (void* b : {c->w0, c->v1, c->v2, c->wa, c->wb})
+        CU(cudaMemsetAsync(b, 0, c->field_bytes, c->stream));
+    c->iteration = 0;
+    CU(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
 int bfg_get_iteration(const bfg_ctx* c, int* it) {
     if (!c || !it) return BFG_EINVAL;
     *it = c->iteration;

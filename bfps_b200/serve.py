@@ -7,10 +7,13 @@ resident on the GPU) and advance together, with the stages of all resident
 requests of the same size batched into one launch per pass.  A tick runs the
 ensemble up to the next event (a resident request reaching its step count,
 or the next arrival as estimated from the measured step time) and
-synchronises once; while it runs, the host polls it (bfg_ens_wait) and
-prepares the inputs of requests that have arrived.  A request that reaches its step count is read back and
-retired, freeing its memory for waiting requests.  Requests that arrive
-while others are running join at the next tick.
+synchronises once; while it runs, the host reads back the requests that
+finished in the previous tick, stages the requests that have arrived (a
+context of their size from a pool of finished ones, reset by
+bfg_ctx_reset, or a new one) and prepares the inputs of later arrivals,
+polling the tick with bfg_ens_wait.  Staged requests join the ensemble at
+the next tick; the memory of finished ones serves later requests of the
+same size, or is freed between ticks for others.
 
 Nothing here computes on the host: every step is bfg_ens_step.
 """
@@ -94,19 +97,64 @@ def prepare(req):
 
 
 class Server:
-    def __init__(self, hbm_budget=150e9, device=0, use_graphs=False, max_tick=64):
+    """Continuous batching over one ensemble.
+
+    The GPU runs ticks (bfg_ens_step over the resident requests) while the
+    host does everything else: reading back the requests that finished in
+    the previous tick (statistics and field downloads on their own
+    contexts' streams), staging newly arrived requests (a context of their
+    size from the pool, or a new one; upload of the initial field; tracers)
+    and preparing the inputs of requests that have arrived.  Membership
+    changes (adding staged requests, removing finished ones) and the release
+    of device memory happen between ticks, when the GPU is idle:
+    cudaFree waits for the whole device.  Memory is reclaimed lazily: the
+    contexts of finished requests serve later requests of their size, and
+    their tracer systems (a few tens of MB; freeing one took 10-30 ms even
+    on an idle GPU) stay allocated, counted in the budget, until memory is
+    needed or the server closes.
+    """
+
+    def __init__(self, hbm_budget=150e9, device=0, use_graphs=False, max_tick=64, pool=True):
         self.budget = hbm_budget
-        self.used = 0
+        self.used = 0              # bytes of running, staged, finishing and pooled requests
         self.device = device
         self.max_tick = max_tick   # most ensemble steps between two synchronisations
         self.step_ms = 0.0         # device time of one ensemble step, last tick
+        self.busy_ms = 0.0         # device time of all ticks
+        self.ticks = 0
         self.ens = ensemble(device)
         self.ens.use_graphs(use_graphs)
-        self.running = {}   # rid -> (request, fs, ps, steps_done)
+        self.running = {}   # rid -> [request, fs, ps, steps_done]
+        self.staged = []    # [request, fs, ps] not yet in the ensemble
+        self.finishing = [] # [request, fs, ps] out of the ensemble, results not yet read
+        self.pool = {} if pool else None   # (n, precision) -> idle contexts
+        self.retired = []   # [particles_system, bytes] of finished requests, not yet freed
         self.done = []
+        # host seconds per phase of run(): step (the bfg_ens_step call:
+        # membership rebuild and launches), collect, admit, wait (the tick
+        # still running), between (memory release, staging and membership
+        # changes while the GPU is idle)
+        self.host_s = dict(step=0.0, collect=0.0, admit=0.0, wait=0.0, between=0.0)
 
-    def _start(self, req, now):
-        fs = vorticity_equation(req.n, precision=req.precision, device=self.device)
+    @staticmethod
+    def _ctx_bytes(n, precision):
+        return request_bytes(n, precision, 0, 0)
+
+    @staticmethod
+    def _tracer_bytes(req):
+        return (request_bytes(req.n, req.precision, req.ntracers, req.nsteps_ab)
+                - request_bytes(req.n, req.precision, 0, 0))
+
+    def _context(self, req):
+        key = (req.n, req.precision)
+        if self.pool is not None and self.pool.get(key):
+            fs = self.pool[key].pop()
+            fs.reset()
+            return fs, False
+        return vorticity_equation(req.n, precision=req.precision, device=self.device), True
+
+    def _stage(self, req, now):
+        fs, fresh = self._context(req)
         fs.nu = req.nu
         fs.forcing_type = "linear"
         fs.famplitude, fs.fk0, fs.fk1 = req.famplitude, req.fk0, req.fk1
@@ -116,14 +164,62 @@ class Server:
         ps = None
         if req.ntracers > 0:
             ps = particles_system(fs, req.pos, req.neighbours, req.smoothness, req.nsteps_ab)
-        self.ens.add(fs, req.dt, ps)
         req.admitted = now
-        self.running[req.rid] = [req, fs, ps, 0]
-        self.used += request_bytes(req.n, req.precision, req.ntracers, req.nsteps_ab)
+        if fresh:
+            self.used += self._ctx_bytes(req.n, req.precision)
+        self.used += self._tracer_bytes(req)
+        self.staged.append([req, fs, ps])
 
-    def _finish(self, rid, now):
-        req, fs, ps, _ = self.running.pop(rid)
-        self.ens.remove(fs)
+    def _admit(self, waiting, now):
+        """Stage waiting requests in arrival order while they fit the budget
+        (a pooled context of the right size costs nothing new)."""
+        still = []
+        for req in waiting:
+            key = (req.n, req.precision)
+            pooled = self.pool is not None and bool(self.pool.get(key))
+            need = self._tracer_bytes(req) + (0 if pooled else self._ctx_bytes(req.n, req.precision))
+            if self.used + need <= self.budget:
+                self._stage(req, now)
+            else:
+                still.append(req)
+        return still
+
+    def _free_tracers(self, fs=None):
+        """Free retired tracer systems (all of them, or those of context fs)."""
+        keep = []
+        for ps, nbytes in self.retired:
+            if fs is None or ps.fs is fs:
+                ps.close()
+                self.used -= nbytes
+            else:
+                keep.append([ps, nbytes])
+        self.retired = keep
+
+    def _release(self, req):
+        """Between ticks: free retired tracer systems, then idle contexts of
+        other sizes, until `req` fits (a pooled context of its own size is
+        kept for it).  A context is freed only after the tracer systems that
+        still refer to it."""
+        key = (req.n, req.precision)
+        pooled = self.pool is not None and bool(self.pool.get(key))
+        need = self._tracer_bytes(req) + (0 if pooled else self._ctx_bytes(*key))
+        if self.used + need <= self.budget:
+            return
+        self._free_tracers()
+        if not self.pool:
+            return
+        for other in list(self.pool):
+            if other == key:
+                continue
+            while self.pool[other] and self.used + need > self.budget:
+                fs = self.pool[other].pop()
+                fs.close()
+                self.used -= self._ctx_bytes(*other)
+
+    def _collect(self, entry, now):
+        """Results of a request out of the ensemble (its own streams), then
+        its context to the pool; its tracers are freed between ticks."""
+        req, fs, ps = entry
         # the final state's statistics (NSVE::do_stats): the energy spectrum
         # E(k) = tr(spec_uu) / 2, summed in a fixed order on the device, so a
         # request gives the same bits alone and in the mix
@@ -133,37 +229,52 @@ class Server:
                       "energy_spectrum": 0.5 * np.einsum("kii->k", spec_uu)}
         if ps is not None:
             req.result["tracers"] = ps.state()[0]
-            ps.close()
-        fs.close()
+            self.retired.append([ps, self._tracer_bytes(req)])
+        else:
+            self.used -= self._tracer_bytes(req)
+        if self.pool is not None:
+            self.pool.setdefault((req.n, req.precision), []).append(fs)
+        else:
+            if ps is not None:
+                self._free_tracers(fs)
+            fs.close()
+            self.used -= self._ctx_bytes(req.n, req.precision)
         req.finished = now
-        self.used -= request_bytes(req.n, req.precision, req.ntracers, req.nsteps_ab)
         self.done.append(req)
+
+    def _between_ticks(self):
+        for req, fs, ps in self.staged:
+            self.ens.add(fs, req.dt, ps)
+            self.running[req.rid] = [req, fs, ps, 0]
+        self.staged = []
 
     def run(self, requests, clock=time.perf_counter, max_wall=None):
         """Serve a stream (arrival times relative to the call).  Returns the
-        finished requests; time-to-completion is finished - arrival."""
+        finished requests; time-to-completion is finished - arrival (the
+        results read back on the host)."""
         pending = sorted(requests, key=lambda r: r.arrival)
         t0 = clock()
         qi = 0
         waiting = []
-        while qi < len(pending) or waiting or self.running:
+        while qi < len(pending) or waiting or self.running or self.staged or self.finishing:
             now = clock() - t0
             if max_wall is not None and now > max_wall:
                 break
             while qi < len(pending) and pending[qi].arrival <= now:
                 waiting.append(pending[qi])
                 qi += 1
-            # admission by HBM budget, in arrival order
-            still = []
-            for req in waiting:
-                need = request_bytes(req.n, req.precision, req.ntracers, req.nsteps_ab)
-                if self.used + need <= self.budget:
-                    self._start(req, clock() - t0)
-                else:
-                    still.append(req)
-            waiting = still
+            # between ticks (the GPU is idle): release what waits for it
+            tb = clock()
+            if waiting:
+                self._release(waiting[0])
+            waiting = self._admit(waiting, clock() - t0)
+            self._between_ticks()
+            self.host_s["between"] += clock() - tb
             if not self.running:
-                if qi < len(pending):
+                for entry in self.finishing:
+                    self._collect(entry, clock() - t0)
+                self.finishing = []
+                if qi < len(pending) and not waiting:
                     time.sleep(max(0.0, min(0.01, pending[qi].arrival - (clock() - t0))))
                 continue
             # one tick: ensemble steps up to the next event -- the first resident
@@ -174,9 +285,24 @@ class Server:
                 until = pending[qi].arrival - (clock() - t0)
                 k = min(k, max(1, int(until * 1e3 / self.step_ms)))
             k = max(1, min(k, self.max_tick))
+            tb = clock()
             self.ens.step(k)
-            # while the tick runs, prepare the inputs of arrived requests
-            # that still need them (host work off the GPU's critical path)
+            tc = clock()
+            self.host_s["step"] += tc - tb
+            # while the tick runs: the previous tick's finished requests,
+            # newly arrived requests (staged for the next tick) and the
+            # inputs of arrived requests
+            for entry in self.finishing:
+                self._collect(entry, clock() - t0)
+            self.finishing = []
+            td = clock()
+            self.host_s["collect"] += td - tc
+            while qi < len(pending) and pending[qi].arrival <= clock() - t0:
+                waiting.append(pending[qi])
+                qi += 1
+            waiting = self._admit(waiting, clock() - t0)
+            te = clock()
+            self.host_s["admit"] += te - td
             while not self.ens.wait(0.002):
                 now = clock() - t0
                 todo = [r for r in waiting + pending[qi:] if r.arrival <= now and r.w0 is None]
@@ -184,18 +310,37 @@ class Server:
                     self.ens.wait()
                     break
                 prepare(todo[0])
-            self.step_ms = self.ens.last_ms() / k
+            tick_ms = self.ens.last_ms()
+            self.host_s["wait"] += clock() - te
+            self.busy_ms += tick_ms
+            self.ticks += 1
+            self.step_ms = tick_ms / k
             for rid in list(self.running):
                 self.running[rid][3] += k
                 if self.running[rid][3] >= self.running[rid][0].steps:
-                    self._finish(rid, clock() - t0)
+                    req, fs, ps, _ = self.running.pop(rid)
+                    self.ens.remove(fs)
+                    self.finishing.append([req, fs, ps])
         return self.done
 
     def close(self):
+        # retired tracer systems first: their contexts may since have been
+        # reused by running or staged requests, and are freed below
+        self._free_tracers()
         for rid in list(self.running):
             req, fs, ps, _ = self.running.pop(rid)
             self.ens.remove(fs)
             if ps is not None:
                 ps.close()
             fs.close()
+        for req, fs, ps in self.staged + self.finishing:
+            if ps is not None:
+                ps.close()
+            fs.close()
+        self.staged, self.finishing = [], []
+        if self.pool:
+            for fss in self.pool.values():
+                for fs in fss:
+                    fs.close()
+            self.pool = {}
         self.ens.close()

@@ -201,6 +201,11 @@ class vorticity_equation:
         check(lib().bfg_check_finite(self._h, fid, ctypes.byref(n)), self._h)
         return n.value
 
+    def reset(self):
+        """bfg_ctx_reset: the state of a new context of this grid (fields
+        zero, iteration 0) on the same device memory."""
+        check(lib().bfg_ctx_reset(self._h), self._h)
+
     def autotune(self, reps=3):
         """bfg_autotune: time both schedules of the IZ, IY, FY and FZ passes
         on this context and keep the faster for this device, grid size and

@@ -141,6 +141,12 @@ int bfg_field_ift(bfg_ctx* ctx, int field_id);
 int bfg_field_stats(bfg_ctx* ctx, const void* field, double max_estimate, int nbins,
                     double* spec, double* mom, int64_t* hist);
 
+/* No counterpart in the reference: returns a context to the state of a new
+ * one of the same grid (every field buffer zero, iteration 0), keeping its
+ * device memory, physics members and tables, so that a server can reuse it
+ * for the next solve of that size without freeing and allocating. */
+int bfg_ctx_reset(bfg_ctx* ctx);
+
 /* iteration counter (vorticity_equation::iteration). */
 int bfg_get_iteration(const bfg_ctx* ctx, int* iteration);
 int bfg_set_iteration(bfg_ctx* ctx, int iteration);
