@@ -169,3 +169,28 @@ def test_serving_results_equal_alone():
         if ps is not None:
             assert np.array_equal(r.result["tracers"], ps.state()[0])
         assert r.finished >= r.admitted >= r.arrival
+
+
+def test_context_reset_equals_new():
+    """bfg_ctx_reset: a context that has run a solve, reset and given a new
+    problem, steps bit for bit like a new context (the serving pool reuses
+    contexts this way)."""
+    from bfps_b200.solver import NSVEparticles_step
+    spec = SPECS[1]  # 32^3 with tracers
+    used, ps_used = _make(SPECS[4], "single")
+    NSVEparticles_step(used, ps_used, SPECS[4][6], 3)
+    ps_used.close() if ps_used is not None else None
+    used.reset()
+    assert used.iteration == 0
+    n, nu, seed, nt, nm, nab, dt = spec
+    used.nu = nu
+    used.set_cvorticity(ic.vorticity_ic(n, seed=seed, dtype=used.cdtype))
+    from bfps_b200.solver import particles_system
+    ps = particles_system(used, ic.tracer_ic(nt, seed=seed), nm[0], nm[1], nab)
+    NSVEparticles_step(used, ps, dt, 4)
+    fresh, ps_fresh = _make(spec, "single")
+    NSVEparticles_step(fresh, ps_fresh, dt, 4)
+    assert np.array_equal(used.get_cvorticity(), fresh.get_cvorticity())
+    assert np.array_equal(ps.state()[0], ps_fresh.state()[0])
+    for obj in (ps, ps_fresh, used, fresh):
+        obj.close()
