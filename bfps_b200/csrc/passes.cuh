@@ -327,33 +327,54 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
 #pragma unroll
         for (int c = 0; c < 3; ++c) tt[c] = zero_c<T>();
     }
-    // RK update (vorticity_equation.cpp:366-434), only for k2 <= kM2
+    // RK update (vorticity_equation.cpp:366-434), only for k2 <= kM2.  The
+    // RK operands are read only where they are used: outside kM2 stages 1-2
+    // write zero and stage 3 keeps v0 (about half of the modes, and the
+    // whole of many tiles' rows, lie outside the smooth filter's sphere)
     const bool inside = k2 <= kp.kM2;
     const T dt = (T)kp.dt;
     cpx<T> o[3];
     const int nfac = nxv + 2 * N;
     if (MODE == CM_FZ_RK1) {
-        const T f0 = fc.fxy0 * fac[nxv + N + l];
+        if (inside) {
+            const T f0 = fc.fxy0 * fac[nxv + N + l];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            o[c] = inside ? mk<T>((v0[c].x + dt * tt[c].x) * f0, (v0[c].y + dt * tt[c].y) * f0)
-                          : zero_c<T>();
+            for (int c = 0; c < 3; ++c) {
+                const cpx<T> a0 = v0[c];
+                o[c] = mk<T>((a0.x + dt * tt[c].x) * f0, (a0.y + dt * tt[c].y) * f0);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
+        }
     } else if (MODE == CM_FZ_RK2) {
-        const T f0 = fc.fxy0 * fac[nfac + nxv + N + l];
-        const T f1 = fc.fxy1 * fac[2 * nfac + nxv + N + l];
+        if (inside) {
+            const T f0 = fc.fxy0 * fac[nfac + nxv + N + l];
+            const T f1 = fc.fxy1 * fac[2 * nfac + nxv + N + l];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            o[c] = inside ? mk<T>((3 * v0[c].x * f0 + (vp[c].x + dt * tt[c].x) * f1) * (T)0.25,
-                                  (3 * v0[c].y * f0 + (vp[c].y + dt * tt[c].y) * f1) * (T)0.25)
-                          : zero_c<T>();
+            for (int c = 0; c < 3; ++c) {
+                const cpx<T> a0 = v0[c], ap = vp[c];
+                o[c] = mk<T>((3 * a0.x * f0 + (ap.x + dt * tt[c].x) * f1) * (T)0.25,
+                             (3 * a0.y * f0 + (ap.y + dt * tt[c].y) * f1) * (T)0.25);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) o[c] = zero_c<T>();
+        }
     } else {
         const T third = (T)(1.0 / 3.0);  // the division by 3 as a product (within one rounding)
-        const T f0 = fc.fxy0 * fac[nfac + nxv + N + l];
+        if (inside) {
+            const T f0 = fc.fxy0 * fac[nfac + nxv + N + l];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            o[c] = inside ? mk<T>((v0[c].x * f0 + 2 * (vp[c].x + dt * tt[c].x)) * f0 * third,
-                                  (v0[c].y * f0 + 2 * (vp[c].y + dt * tt[c].y)) * f0 * third)
-                          : v0[c];
+            for (int c = 0; c < 3; ++c) {
+                const cpx<T> a0 = v0[c], ap = vp[c];
+                o[c] = mk<T>((a0.x * f0 + 2 * (ap.x + dt * tt[c].x)) * f0 * third,
+                             (a0.y * f0 + 2 * (ap.y + dt * tt[c].y)) * f0 * third);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) o[c] = v0[c];
+        }
         // final force_divfree of the state (vorticity_equation.cpp:436)
         if (k2 > 0.0) divfree<T>(fc.kxT, fc.kyT, kzT, ik2, o);
         if (kzero) {
@@ -502,11 +523,16 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         }
         if constexpr (NRK > 0) {
             // RK operands of this tile, rows S[ky=a][kz=l][kx0..kx0+TKX): into
-            // L2 while the tile is transformed, read by the epilogue
+            // L2 while the tile is transformed, read by the epilogue; only
+            // rows with a mode inside kM2, except v0 in stage 3, which the
+            // epilogue also reads outside
             const int a = tl / ntx;
             const int kx0 = (tl % ntx) * TKX;
             const cpx<T>* rk_v0 = mbuf(mem[m], rl.v0);  // mb is not yet visible to all
             const cpx<T>* rk_vp = NRK > 1 ? mbuf(mem[m], rl.vp) : rk_v0;
+            const KParams& gkp = mem[m].kp;
+            const double kyv = kwrap<N>(a, gkp.dky), kxv = (double)kx0 * gkp.dkx;
+            const double room = gkp.kM2 - (kxv * kxv + kyv * kyv);  // kz^2 left inside
             constexpr int LINES = (3 * TKX * (int)sizeof(cpx<T>) + 127) / 128 + 1;
             const int nbytes = 3 * min(TKX, NXV - kx0) * (int)sizeof(cpx<T>);
             for (int e = tid; e < N * NRK * LINES; e += NT) {
@@ -514,6 +540,9 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 const int r = e / LINES;
                 const int arr = r % NRK;
                 const int l = r / NRK;
+                const double kz = kwrap<N>(l, gkp.dkz);
+                const bool used = (MODE == CM_FZ_RK3 && arr == 0) || kz * kz <= room;
+                if (!used) continue;
                 const char* row = reinterpret_cast<const char*>(
                     ((arr == 0) ? rk_v0 : rk_vp) + ((size_t)a * N + l) * nxp3 + (size_t)kx0 * 3);
                 if (128 * q < nbytes) prefetch_l2(row + 128 * q);
