@@ -386,6 +386,21 @@ __device__ __forceinline__ void fz_point(const KParams& kp, const cpx<T>* tile, 
     for (int c = 0; c < 3; ++c) out0[pt * 3 + c] = o[c];
 }
 
+// An RK tile of the FZ pass (one ky, kx columns kx0..) whose every mode lies
+// outside kM2 (kx0^2 + ky^2 > kM2): its epilogue writes zero (stages 1-2) or
+// keeps v0 (stage 3) without reading the transformed product, so neither the
+// product's load nor its transform is needed (about a fifth of the tiles
+// with the smooth filter's kM = N/2 - 1).
+template <int N, int MODE>
+__device__ __forceinline__ bool fz_tile_outside(const KParams& kp, int a, int kx0) {
+    if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
+        const double ky = kwrap<N>(a, kp.dky), kx = (double)kx0 * kp.dkx;
+        return kx * kx + ky * ky > kp.kM2;
+    } else {
+        return false;
+    }
+}
+
 template <typename T, int N, int MODE, int S>
 __device__ __forceinline__ void col_issue_load(cpx<T>* tile, const cpx<T>* in0,
                                                const cpx<T>* in1, int a, int kx0, int ncol,
@@ -506,8 +521,9 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
     if (t < ntiles) {
         const int m = t / tiles_per, tl = t - m * tiles_per;
         const int kx0 = (tl % ntx) * TKX;
-        col_issue_load<T, N, MODE, S>(bufs, mbuf(mem[m], rl.in0), mbuf(mem[m], rl.in1), tl / ntx, kx0,
-                                   min(TKX, NXV - kx0), nxp3, tid);
+        if (!fz_tile_outside<N, MODE>(mem[m].kp, tl / ntx, kx0))
+            col_issue_load<T, N, MODE, S>(bufs, mbuf(mem[m], rl.in0), mbuf(mem[m], rl.in1), tl / ntx,
+                                          kx0, min(TKX, NXV - kx0), nxp3, tid);
     }
     cp_async_commit();
     __shared__ Member<T> mb;  // this tile's member, read once per tile
@@ -554,9 +570,10 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             if (tn < ntiles) {
                 const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
                 const int kx0n = (tln % ntx) * TKX;
-                col_issue_load<T, N, MODE, S>(bufs + ((it + 1) & 1) * TILE, mbuf(mem[mn], rl.in0),
-                                           mbuf(mem[mn], rl.in1), tln / ntx, kx0n,
-                                           min(TKX, NXV - kx0n), nxp3, tid);
+                if (!fz_tile_outside<N, MODE>(mem[mn].kp, tln / ntx, kx0n))
+                    col_issue_load<T, N, MODE, S>(bufs + ((it + 1) & 1) * TILE, mbuf(mem[mn], rl.in0),
+                                                  mbuf(mem[mn], rl.in1), tln / ntx, kx0n,
+                                                  min(TKX, NXV - kx0n), nxp3, tid);
             }
             cp_async_commit();
         }
@@ -644,8 +661,12 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
         constexpr int MR = col_mr<T, MODE, S>();
         constexpr int NST = plan_nstages(N, MR);
         if constexpr (MODE >= CM_FZ_RK1 && MODE <= CM_FZ_RK3) {
-            if (ncol == TKX) dif<T, N, INV, P, LY, 1, N, MR>(tile, tw, tid, NT);
-            else dif<T, N, INV, PN, LYN, 1, N, MR>(tile, tw, tid, NT);
+            // a tile wholly outside kM2 was not loaded: its epilogue reads
+            // only the RK operands (fz_tile_outside)
+            if (!fz_tile_outside<N, MODE>(kp, a, kx0)) {
+                if (ncol == TKX) dif<T, N, INV, P, LY, 1, N, MR>(tile, tw, tid, NT);
+                else dif<T, N, INV, PN, LYN, 1, N, MR>(tile, tw, tid, NT);
+            }
             __syncthreads();
             // ---- epilogue: one thread per mode (kz = l, kx = kx0 + col)
             const double ky = kwrap<N>(a, kp.dky);
@@ -686,8 +707,9 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
             if (tn < ntiles) {
                 const int mn = tn / tiles_per, tln = tn - mn * tiles_per;
                 const int kx0n = (tln % ntx) * TKX;
-                col_issue_load<T, N, MODE, S>(bufs, mbuf(mem[mn], rl.in0), mbuf(mem[mn], rl.in1),
-                                           tln / ntx, kx0n, min(TKX, NXV - kx0n), nxp3, tid);
+                if (!fz_tile_outside<N, MODE>(mem[mn].kp, tln / ntx, kx0n))
+                    col_issue_load<T, N, MODE, S>(bufs, mbuf(mem[mn], rl.in0), mbuf(mem[mn], rl.in1),
+                                                  tln / ntx, kx0n, min(TKX, NXV - kx0n), nxp3, tid);
             }
             cp_async_commit();
             t = tn;
