@@ -99,7 +99,7 @@ def algorithmic_bytes(cfg):
 # divided by its algorithmic bytes, from the ncu captures summarised under
 # profiles/ (256^3 FP32 passes; tracer kernel at 4e6 tracers on 256^3).
 # Traffic at another size is taken to scale with the algorithmic bytes.
-TRAFFIC_RATIO = {"X": 0.951, "IZ": 0.931, "IY": 0.948, "FY": 0.886, "FZ": 1.035, "tracers": 0.983}
+TRAFFIC_RATIO = {"X": 0.951, "IZ": 0.931, "IY": 0.948, "FY": 0.886, "FZ": 0.744, "tracers": 0.983}
 
 
 class ClockSampler:
