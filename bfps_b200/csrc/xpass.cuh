@@ -358,6 +358,10 @@ struct Cfg {
     static constexpr int RL = (N / 2 + 4) * 3;     // padded interleaved row (complex)
     static constexpr int XB = G == 4 ? 68 : (G == 8 ? 72 : 144);  // exchange block per row
     static constexpr int P1 = G == 16 ? 18 : 9;                   // [n1][l] pitch
+    // twiddle table [n1][l] pitch: the forward transform of G = 16 reads it
+    // with lane 2 n1 + l1 at column l1 + 2 l2, which a pitch of 16 would put
+    // on one bank for all eight n1
+    static constexpr int TP = G == 16 ? 18 : G;
 };
 
 template <int N>
@@ -374,7 +378,7 @@ __device__ __forceinline__ void inv_g(cpx<float> (&v)[8], cpx<float>* xb,
     constexpr int G = Cfg<N>::G, P1 = Cfg<N>::P1;
     dft<float, true, 8>(v);  // over q -> n1
 #pragma unroll
-    for (int n1 = 1; n1 < 8; ++n1) v[n1] = cmulc(v[n1], t1[n1 * G + l]);  // W_M^{-n1 l}
+    for (int n1 = 1; n1 < 8; ++n1) v[n1] = cmulc(v[n1], t1[n1 * Cfg<N>::TP + l]);  // W_M^{-n1 l}
     __syncwarp();
 #pragma unroll
     for (int n1 = 0; n1 < 8; ++n1) xb[n1 * P1 + l] = v[n1];
@@ -437,8 +441,8 @@ __device__ __forceinline__ void fwd_g(cpx<float> (&v)[8], cpx<float>* xb,
         dft<float, false, 4>(b);
 #pragma unroll
         for (int k = 1; k < 4; ++k) {
-            a[k] = cmul(a[k], t1[l * G + k]);        // W_M^{n1 k}
-            b[k] = cmul(b[k], t1[(l + 4) * G + k]);
+            a[k] = cmul(a[k], t1[l * Cfg<N>::TP + k]);        // W_M^{n1 k}
+            b[k] = cmul(b[k], t1[(l + 4) * Cfg<N>::TP + k]);
         }
         __syncwarp();
 #pragma unroll
@@ -449,7 +453,7 @@ __device__ __forceinline__ void fwd_g(cpx<float> (&v)[8], cpx<float>* xb,
     } else if constexpr (G == 8) {
         dft<float, false, 8>(v);  // over n2 -> k (lane = n1)
 #pragma unroll
-        for (int k = 1; k < 8; ++k) v[k] = cmul(v[k], t1[k * G + l]);  // W_M^{n1 k}, n1 = l
+        for (int k = 1; k < 8; ++k) v[k] = cmul(v[k], t1[k * Cfg<N>::TP + l]);  // W_M^{n1 k}, n1 = l
         __syncwarp();
 #pragma unroll
         for (int k = 0; k < 8; ++k) xb[l * P1 + k] = v[k];
@@ -468,7 +472,7 @@ __device__ __forceinline__ void fwd_g(cpx<float> (&v)[8], cpx<float>* xb,
         for (int m1 = 0; m1 < 8; ++m1) v[m1] = xb[n1 * P1 + 9 * l1 + m1];
         dft<float, false, 8>(v);  // over m1 -> l2
 #pragma unroll
-        for (int l2 = 0; l2 < 8; ++l2) v[l2] = cmul(v[l2], t1[n1 * G + l1 + 2 * l2]);  // W_M^{n1 k}
+        for (int l2 = 0; l2 < 8; ++l2) v[l2] = cmul(v[l2], t1[n1 * Cfg<N>::TP + l1 + 2 * l2]);  // W_M^{n1 k}
         __syncwarp();
 #pragma unroll
         for (int l2 = 0; l2 < 8; ++l2) xb[n1 * P1 + l1 + 2 * l2] = v[l2];
@@ -492,7 +496,7 @@ __device__ __forceinline__ int grid_pair(int l, int i) {
 template <int N>
 __host__ __device__ constexpr size_t xwg_smem_bytes() {
     return (size_t)xwg::NWARP * sizeof(xwg::Smem<N>) +
-           (size_t)(N + 8 * xwg::Cfg<N>::G) * sizeof(cpx<float>) + xwg::NWARP * 16;
+           (size_t)(N + 8 * xwg::Cfg<N>::TP) * sizeof(cpx<float>) + xwg::NWARP * 16;
 }
 
 template <int N, bool WRITE_RU>
@@ -513,14 +517,14 @@ row_nonlin_wg(const Member<float>* __restrict__ mem, const Roles rl,
     extern __shared__ __align__(128) unsigned char xwg_smem_raw[];
     Smem<N>* ws = reinterpret_cast<Smem<N>*>(xwg_smem_raw);
     C* tw = reinterpret_cast<C*>(ws + NWARP);  // exp(-2 pi i m / N), m < N
-    C* t1 = tw + N;                            // [n1][l] = W_M^{n1 l}
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(t1 + 8 * G);
+    C* t1 = tw + N;                            // [n1][l] = W_M^{n1 l}, pitch TP
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(t1 + 8 * CF::TP);
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < N; i += blockDim.x) tw[i] = tw_g[i];
     for (int i = tid; i < 8 * G; i += blockDim.x) {
         const int n1 = i / G, l = i % G;
-        t1[i] = tw_g[(2 * n1 * l) % N];
+        t1[n1 * CF::TP + l] = tw_g[(2 * n1 * l) % N];
     }
     if (tid < 2 * NWARP) mbar_init(&bars[tid], 1);
     fence_mbar_init();
@@ -533,9 +537,13 @@ row_nonlin_wg(const Member<float>* __restrict__ mem, const Roles rl,
     const float inv_np = 1.0f / ((float)N * (float)N * (float)N);
     const int nblk = nrows / Q;  // Q divides N^2: blocks never straddle members
     const int gw = blockIdx.x * NWARP + wid, nw = gridDim.x * NWARP;
-    const int rr_ = lane / G;    // this lane's row in the block
-    const int l = lane % G;      // its lane in the row
-    C* xb = S.x + rr_ * XB;
+    // this lane's row in the block and its lane in the row; G = 8 puts rows
+    // 0, 2 (and 1, 3) in one half-warp: 2 RL apart (8 modulo 16), so the
+    // strided row accesses of the two rows (3 k + c) fall on distinct banks
+    const int grp = lane / G;
+    const int rr_ = G == 8 ? (grp & 1) * 2 + (grp >> 1) : grp;
+    const int l = lane % G;
+    C* xb = S.x + grp * XB;      // exchange block of this lane group
     auto block_src = [&](int blk, int b) -> const C* {
         const int row0 = blk * Q;
         const int m = row0 / rows_per;
