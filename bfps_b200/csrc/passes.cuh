@@ -633,12 +633,18 @@ col_pass(const Member<T>* __restrict__ mem, const Roles rl, const cpx<T>* __rest
                 for (int c = 0; c < 3; ++c) tile[l * PR + col * 3 + c] = u[c];
             };
             if constexpr (NT % TKX == 0) {
-                // a thread keeps one column
-                const int col = tid % TKX;
+                // a thread keeps one column.  In FP32, with a tile pitch of
+                // 2 modulo 4, each half-warp takes eight consecutive rows of
+                // two columns: the 8-byte accesses PR l + 3 col (+ c) then
+                // fall on sixteen distinct banks (with the column fastest
+                // they met two-way)
+                constexpr bool ROWS8 = sizeof(T) == 4 && TKX >= 2 && PR % 4 == 2 && NT % (8 * TKX) == 0;
+                const int col = ROWS8 ? (tid >> 3) % TKX : tid % TKX;
+                const int l0 = ROWS8 ? (tid & 7) + 8 * (tid / (8 * TKX)) : tid / TKX;
                 if (col < ncol) {
                     const double kx = (double)(kx0 + col) * kp.dkx;
                     const double kxy2 = kx * kx + ky * ky;
-                    for (int l = tid / TKX; l < N; l += NT / TKX) point(col, l, kxy2, (T)kx, (T)ky);
+                    for (int l = l0; l < N; l += NT / TKX) point(col, l, kxy2, (T)kx, (T)ky);
                 }
             } else {
                 for (int e = tid; e < N * TKX; e += NT) {
