@@ -385,14 +385,7 @@ def run_ours(args, cfg):
         "vs_baseline": None,
         "dtype": "f32" if cfg["precision"] == "single" else "f64",
         "data": "synthetic (seeded k^4 exp(-2(k/k0)^2) spectrum, uniform tracers)",
-        "config": {"workload": args.workload + ": %d^3 %s, nu=%g, dt=%g, k0=%g, %d tracers "
-                   "(n=%d, m=%d), AB%d, linear forcing 1.5<=|k|<=3" % (
-                       cfg["n"], "fp32" if cfg["precision"] == "single" else "fp64",
-                       cfg["nu"], cfg["dt"], cfg["k0"], cfg["ntracers"], cfg["neighbours"],
-                       cfg["smoothness"], cfg["nsteps_ab"]),
-                   "grid": cfg["n"], "tracers": cfg["ntracers"],
-                   "parallelism": "replicas x%d" % world,
-                   "l2": "inputs larger than L2 (one 3-vector field is %.2f GB)" % (3 * U / 1e9)},
+        "config": workload_config(args, cfg, world),
         "roofline": roof,
         "step_roofline": {"bytes_per_step": step_bytes, "achieved": round(step_ach, 1),
                           "peak": peak, "unit": "GB/s", "frac": round(step_ach / peak, 4),
@@ -758,6 +751,19 @@ def cpu_baseline(cfg, w0, pos, device):
     return base, cmp
 
 
+def workload_config(args, cfg, world):
+    """The `config` of a single-instance workload's line (both arms)."""
+    U = cfg["n"] * cfg["n"] * (cfg["n"] + 2) * (4 if cfg["precision"] == "single" else 8)
+    return {"workload": args.workload + ": %d^3 %s, nu=%g, dt=%g, k0=%g, %d tracers "
+                        "(n=%d, m=%d), AB%d, linear forcing 1.5<=|k|<=3" % (
+                            cfg["n"], "fp32" if cfg["precision"] == "single" else "fp64",
+                            cfg["nu"], cfg["dt"], cfg["k0"], cfg["ntracers"], cfg["neighbours"],
+                            cfg["smoothness"], cfg["nsteps_ab"]),
+            "grid": cfg["n"], "tracers": cfg["ntracers"],
+            "parallelism": "replicas x%d" % world,
+            "l2": "inputs larger than L2 (one 3-vector field is %.2f GB)" % (3 * U / 1e9)}
+
+
 def run_reference(args, cfg):
     """The reference's CPU path on the host cores.  Its own build needs
     FFTW3, HDF5 and MPI, absent here and on the GPU box, so this is the
@@ -791,7 +797,7 @@ def run_reference(args, cfg):
         "warmup": min(1, args.warmup), "ms_per_step": round(s * 1e3, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded k^4 exp(-2(k/k0)^2) spectrum, uniform tracers)",
-        "config": {"workload": args.workload, "grid": cfg["n"], "tracers": cfg["ntracers"]},
+        "config": workload_config(args, cfg, 1),
         "impl": "reference",
         "cpu_baseline": {"value": round(1.0 / s, 6), "unit": "steps/s", "cores": threads,
                          "kind": "port", "cpu_model": cpu_model(),
