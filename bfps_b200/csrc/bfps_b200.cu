@@ -362,12 +362,8 @@ struct Engine {
         const int ntiles = tiles_per * nmem;
         const int grid = std::min(ntiles, c->nsm * col_ctas<T, N, MODE, S>());
         Prof pr(c, col_kind(MODE));
-        // dynamic tile order for the IZ passes with at least 8 tiles per CTA
-        // (and for the FZ stage passes, whose tiles wholly outside kM cost
-        // a fraction of the others)
-        constexpr bool iz = MODE == CM_IZ_VEL || MODE == CM_IZ_PLAIN || MODE == CM_IZ_U;
-        constexpr bool fz = MODE == CM_FZ_RK1 || MODE == CM_FZ_RK2 || MODE == CM_FZ_RK3;
-        int* tctr = ((iz || fz) && ntiles >= 8 * grid) ? c->tctr : nullptr;
+        // dynamic tile order where a launch has at least 8 tiles per CTA
+        int* tctr = ntiles >= 8 * grid ? c->tctr : nullptr;
         kern<<<grid, col_threads<T, N, MODE, S>(), smem, c->stream>>>(mem, rl, (const C*)c->tw, ntx,
                                                                      tiles_per, ntiles, tctr);
         return after_launch(c, "col_pass");
