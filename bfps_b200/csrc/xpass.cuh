@@ -45,6 +45,9 @@ constexpr int XP1 = 36;                // exchange [n1][l] row pitch
 constexpr int XP2 = 68, XQ2 = 17;      // exchange [n1][l1][m1] pitches
 constexpr int XBUF = 8 * XP2;          // 544 >= 8 * XP1, >= 256
 constexpr int T1P = 36;                // twiddle table [n1][l] row pitch
+constexpr int T2P = 9;                 // twiddle table [l1][m1] row pitch: the inverse
+                                       // reads it with l1 over the lanes, which a
+                                       // pitch of 8 puts on two banks for four rows
 
 template <int N>
 struct Smem {
@@ -70,7 +73,7 @@ __device__ __forceinline__ void inv256(cpx<float> (&v)[8], cpx<float>* xb,
     for (int l2 = 0; l2 < 8; ++l2) v[l2] = xb[n1 * XP1 + l1 + 4 * l2];
     dft<float, true, 8>(v);  // over l2 -> m1
 #pragma unroll
-    for (int m1 = 1; m1 < 8; ++m1) v[m1] = cmulc(v[m1], t2[l1 * 8 + m1]);  // W_32^{-l1 m1}
+    for (int m1 = 1; m1 < 8; ++m1) v[m1] = cmulc(v[m1], t2[l1 * T2P + m1]);  // W_32^{-l1 m1}
     __syncwarp();
 #pragma unroll
     for (int m1 = 0; m1 < 8; ++m1) xb[n1 * XP2 + l1 * XQ2 + m1] = v[m1];
@@ -106,8 +109,8 @@ __device__ __forceinline__ void fwd256(cpx<float> (&v)[8], cpx<float>* xb,
     dft<float, false, 4>(b);
 #pragma unroll
     for (int l1 = 1; l1 < 4; ++l1) {
-        a[l1] = cmul(a[l1], t2[l1 * 8 + j]);      // W_32^{m1 l1}, m1 = j
-        b[l1] = cmul(b[l1], t2[l1 * 8 + j + 4]);  // m1 = j + 4
+        a[l1] = cmul(a[l1], t2[l1 * T2P + j]);      // W_32^{m1 l1}, m1 = j
+        b[l1] = cmul(b[l1], t2[l1 * T2P + j + 4]);  // m1 = j + 4
     }
     __syncwarp();
 #pragma unroll
@@ -139,7 +142,7 @@ __device__ __forceinline__ void fwd256(cpx<float> (&v)[8], cpx<float>* xb,
 template <int N>
 __host__ __device__ constexpr size_t xw_smem_bytes() {
     return (size_t)xw::NWARP * sizeof(xw::Smem<N>) +
-           (size_t)(N + 8 * xw::T1P + 32) * sizeof(cpx<float>) + xw::NWARP * 16;
+           (size_t)(N + 8 * xw::T1P + 4 * xw::T2P) * sizeof(cpx<float>) + xw::NWARP * 16;
 }
 
 template <int N, bool WRITE_RU>
@@ -160,8 +163,8 @@ row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
     Smem<N>* ws = reinterpret_cast<Smem<N>*>(xw_smem_raw);
     C* tw = reinterpret_cast<C*>(ws + NWARP);  // exp(-2 pi i m / N), m < N
     C* t1 = tw + N;                            // [n1][l] = W_256^{n1 l}, pitch 36
-    C* t2 = t1 + 8 * T1P;                      // [l1][m1] = W_32^{l1 m1}
-    unsigned long long* bars = reinterpret_cast<unsigned long long*>(t2 + 32);
+    C* t2 = t1 + 8 * T1P;                      // [l1][m1] = W_32^{l1 m1}, pitch T2P
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(t2 + 4 * T2P);
 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int i = tid; i < N; i += blockDim.x) tw[i] = tw_g[i];
@@ -169,7 +172,7 @@ row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
         const int n1 = i >> 5, l = i & 31;
         t1[n1 * T1P + l] = tw_g[(2 * n1 * l) % N];
     }
-    if (tid < 32) t2[tid] = tw_g[16 * ((tid >> 3) * (tid & 7))];
+    if (tid < 32) t2[(tid >> 3) * T2P + (tid & 7)] = tw_g[16 * ((tid >> 3) * (tid & 7))];
     if (tid < 2 * NWARP) mbar_init(&bars[tid], 1);
     fence_mbar_init();
     __syncthreads();
