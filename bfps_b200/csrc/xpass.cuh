@@ -223,16 +223,20 @@ row_nonlin_warp(const Member<float>* __restrict__ mem, const Roles rl,
         for (int f = 0; f < 6; ++f) {
             if (f == 3) {
                 if constexpr (WRITE_RU) {
-                    // u(t) in real space, [x][c] interleaved, through su
+                    // u(t) in real space, [x][c] interleaved, through su.
+                    // Lanes j and j + 2 hold grid pairs 16 apart (96 words,
+                    // one bank): lanes j >= 2 store their odd x first, so
+                    // that each store's 32 words fall on distinct banks
                     float* rr = reinterpret_cast<float*>(S.su);
+                    const int hi = j >= 2 ? 1 : 0;
                     __syncwarp();
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
                         const int n = n1 + 8 * (i < 4 ? j : j + 4) + 64 * (i & 3);
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
-                            rr[(2 * n) * 3 + c] = U[c][i].x;
-                            rr[(2 * n + 1) * 3 + c] = U[c][i].y;
+                            rr[(2 * n + hi) * 3 + c] = hi ? U[c][i].y : U[c][i].x;
+                            rr[(2 * n + 1 - hi) * 3 + c] = hi ? U[c][i].x : U[c][i].y;
                         }
                     }
                     fence_proxy_async();  // this lane's writes, visible to the bulk copy
