@@ -36,7 +36,7 @@ def _worker(rank, world, port, out):
 
 def test_two_gloo_replicas():
     world = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()  # no fork of this multi-threaded process
     out = mgr.dict()
     mp.spawn(_worker, args=(world, _free_port(), out), nprocs=world, join=True)
     (m0, r0, f0), (m1, r1, f1) = out[0], out[1]
